@@ -1,0 +1,159 @@
+/*
+ * ibpm_b200.h -- C ABI of libibpm_b200.so, a CUDA (sm_100a) implementation of
+ * ImmersedBodies.jl's CNAB/IBPM time step.
+ *
+ * The entry points are what a Julia `AbstractSolver` (src/solver.jl:6-28)
+ * binds with `ccall`; see INTEGRATION.md for the Julia and Python stubs.
+ *
+ *   reference interface                         replaced by
+ *   ------------------------------------------  -------------------------------
+ *   CnabSolver(state; fftw, cg)                 ibpm_create + ibpm_set_state
+ *     src/solver.jl:84-150, 152
+ *   advance!(::CnabSolver) src/solver.jl:155    ibpm_advance
+ *   getstate(::CnabSolver) src/solver.jl:153    ibpm_get_state (lazy copy-back)
+ *   update_vars!/boundary_total_force           ibpm_get_forces
+ *     src/problem.jl:676-685, 853-856
+ *   error("Panel index=... outside allowed      IBPM_ERR_REGION + ibpm_last_error
+ *     region") src/coupling.jl:39-41
+ *   save_state/load_state src/io/io.jl:14-71    ibpm_get_state/ibpm_set_state
+ *                                               (same arrays, same layouts)
+ *
+ * Arrays are FP64 in the reference's Julia layouts (column-major, x fastest):
+ *   q, q0      : nq x nlevel, nq = (nx+1)*ny + nx*(ny+1)  (u block, then v block)
+ *   gamma, psi : ng x nlevel, ng = (nx-1)*(ny-1)
+ *   nonlin1/2  : ng x nlevel   (state.nonlin[1], state.nonlin[2])
+ *   xb, ub     : npanel x 2,  ds : npanel,  fbt : 2*npanel (state.F̃b),  fb : npanel x 2
+ * Caller buffers are copied in or out during the call and never retained.
+ * The library owns all device memory and one CUDA stream per handle.
+ * One host thread may use a handle at a time; handles are independent.
+ *
+ * Every call returns IBPM_OK (0), a positive warning, or a negative error.
+ * The message of the last error is kept per handle (ibpm_last_error).
+ */
+#ifndef IBPM_B200_H
+#define IBPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IBPM_ABI_VERSION 1
+
+/* status codes */
+#define IBPM_OK 0
+#define IBPM_WARN_CG_MAXITER 1      /* CG hit maxiter (the reference's cg! is silent) */
+#define IBPM_ERR_INVALID (-1)       /* bad argument or unsupported problem */
+#define IBPM_ERR_CUDA (-2)          /* CUDA runtime error or no device */
+#define IBPM_ERR_REGION (-3)        /* panel outside allowed region (coupling.jl:39-41) */
+#define IBPM_ERR_NOMEM (-4)         /* device allocation failed */
+#define IBPM_ERR_NONFINITE (-5)     /* NaN/Inf met in the CG residual */
+
+/* body kinds (src/problem.jl:226-258) */
+#define IBPM_BODY_STATIC 0          /* StaticBody */
+#define IBPM_BODY_MOVING_RIGID 1    /* MovingRigidBody */
+
+/* precision modes */
+#define IBPM_FP64 0                 /* plain FP64 drop-in path */
+
+typedef struct ibpm_problem {
+    int32_t nx, ny, nlevel;     /* MultiDomainGrid base.n and nlevel (problem.jl:398-409) */
+    double h, x0, y0;           /* base.h, base.x0 */
+    double Re;                  /* Fluid.Re */
+    double dt;                  /* CNAB.dt */
+    int32_t npanel;             /* n_panels(bodies) */
+    int32_t nbody;              /* number of preset bodies, in Bodies order */
+    const int32_t *body_kind;   /* nbody entries, IBPM_BODY_* */
+    const int32_t *body_start;  /* nbody+1 panel offsets (0-based), panel_range of each body */
+    const double *body_xb;      /* bodypanels(body).xb stacked, npanel x 2 column-major */
+    const double *body_ds;      /* bodypanels(body).ds stacked, npanel */
+    int32_t grid_moving;        /* 0: StaticGrid, 1: MovingGrid (fluid.jl:22-67) */
+} ibpm_problem;
+
+typedef struct ibpm_options {
+    int32_t precision;          /* IBPM_FP64 */
+    int32_t device;             /* CUDA device ordinal */
+    int32_t cg_maxiter;         /* cg kwargs (solver.jl:137): maxiter, default 5000 */
+    double cg_reltol;           /* default 1e-12 */
+    double cg_abstol;           /* default 0 */
+} ibpm_options;
+
+/* Host-callback results for one step, evaluated by the caller at that step's t. */
+typedef struct ibpm_step_params {
+    double freestream[2];       /* fluid.freestream_vel(t) */
+    double grid_motion[6];      /* GridVelocity: center(2), vel(2), angle, angular_vel */
+    const double *body_motion;  /* nbody x 6 row-major: RigidBodyTransform pos(2), vel(2),
+                                   angle, angular_vel; entries of static bodies are ignored;
+                                   may be NULL when no body moves */
+} ibpm_step_params;
+
+/* A view of State (src/problem.jl:626-639).  NULL array pointers are skipped. */
+typedef struct ibpm_state_view {
+    int64_t index;
+    double t0;
+    double *q, *q0, *gamma, *psi, *nonlin1, *nonlin2;
+    double *xb, *ds, *ub, *fbt;
+    double freestream[2];
+} ibpm_state_view;
+
+typedef struct ibpm_info {
+    int64_t nq, ng, nbc;        /* GridIndices sizes (problem.jl:374-388) */
+    int32_t static_bodies;      /* 1: precomputed B^-1, 0: CG every step */
+    int32_t last_cg_iters;      /* iterations of the last step's CG (0 for static bodies) */
+    double last_cg_residual;    /* final ||r|| of that CG */
+    int64_t device_bytes;       /* device memory held by the handle */
+} ibpm_info;
+
+typedef struct ibpm_handle ibpm_handle;
+
+/* Fills the reference defaults: FP64, device 0, maxiter 5000, reltol 1e-12, abstol 0. */
+void ibpm_default_options(ibpm_options *opt);
+
+/* CnabSolver(State(prob)) (solver.jl:84-150): allocates, computes the panel weights
+ * of static bodies (errors with IBPM_ERR_REGION like coupling.jl:39-41), the
+ * A/Ainv operators and, for static bodies, B and B^-1 on the device.  The state
+ * starts as State(prob) (problem.jl:640-665): zeros, index 0, t0 = 0.
+ * On failure *out is NULL and ibpm_last_error(NULL) gives the message. */
+int ibpm_create(const ibpm_problem *prob, const ibpm_options *opt, ibpm_handle **out);
+void ibpm_destroy(ibpm_handle *h);
+
+/* Upload/download State arrays.  set_state recomputes t from index and t0
+ * (set_time_index!, problem.jl:705-708) and fb (update_vars!). */
+int ibpm_set_state(ibpm_handle *h, const ibpm_state_view *st);
+int ibpm_get_state(ibpm_handle *h, ibpm_state_view *st);
+
+/* advance!(solver) nsteps times; params[k] holds the callbacks at step k.  Returns
+ * after the device finished the steps.  IBPM_WARN_CG_MAXITER if any CG stopped at maxiter. */
+int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params);
+
+/* state.fb (npanel x 2) and boundary_total_force over all panels (2); NULL skips. */
+int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force);
+
+int ibpm_get_time(ibpm_handle *h, int64_t *index, double *t);
+int ibpm_get_info(ibpm_handle *h, ibpm_info *info);
+const char *ibpm_last_error(const ibpm_handle *h);
+
+/* The library's CUDA stream (cudaStream_t) for callers that time on it. */
+void *ibpm_stream(ibpm_handle *h);
+/* Number of kernels this handle launched so far (instrumentation). */
+int64_t ibpm_kernel_launches(const ibpm_handle *h);
+
+/* Kernel timing (instrumentation for roofline reports): when enabled, every
+ * launch of the classes below is bracketed by CUDA events on the handle's
+ * stream.  ibpm_profile(h, 1) clears the counters; ibpm_profile_read gives the
+ * launches, summed device time (ms) and algorithmic bytes (one read of each
+ * input field and one write of each output field) of a class. */
+#define IBPM_KCLASS_XPASS 0         /* DST along x (row pass) */
+#define IBPM_KCLASS_YPASS 1         /* DST along y, spectral multiply, DST along y */
+#define IBPM_KCLASS_NONLINEAR 2     /* nonlinear advection term */
+#define IBPM_KCLASS_CURL 3          /* curl of the streamfunction */
+#define IBPM_KCLASS_COUNT 4
+int ibpm_profile(ibpm_handle *h, int enable);
+int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms, double *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,137 @@
+"""FP64 GPU path (libibpm_b200.so through its C ABI) against the CPU oracle and
+the golden fixtures.  Tolerances: vorticity (Γ) relative L2 <= 1e-10 and force
+coefficients <= 1e-9 relative to the largest force, as the drop-in requires."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from fixtures import problem_from_fixture, rel_l2
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+FIXTURES = sorted(p for p in glob.glob(os.path.join(GOLD, "*.npz")) if "dst1" not in p and "delta" not in p)
+
+TOL_GAMMA = 1e-10
+TOL_FORCE = 1e-9
+
+
+def _run_gpu(ib, state, nsteps):
+    s = ib.create_solver(state)
+    forces = []
+    for _ in range(nsteps):
+        s.advance_()
+        forces.append(state.fb.sum(axis=0).copy())
+    s.getstate()
+    return s, np.array(forces)
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
+def test_gpu_matches_golden(ib, path):
+    fx = np.load(path)
+    prob, st = problem_from_fixture(ib, fx)
+    s, forces = _run_gpu(ib, st, int(fx["nsteps"]))
+    assert rel_l2(st.Gamma, fx["Gamma"]) <= TOL_GAMMA
+    assert rel_l2(st.psi, fx["psi"]) <= TOL_GAMMA
+    assert rel_l2(st.q, fx["q"]) <= TOL_GAMMA
+    assert rel_l2(st.nonlin[1], fx["nonlin2"]) <= TOL_GAMMA
+    assert np.abs(forces - fx["forces"]).max() <= TOL_FORCE * np.abs(fx["forces"]).max()
+    if "cg_iters" in fx:
+        assert abs(s.info().last_cg_iters - int(fx["cg_iters"])) <= 1
+
+
+def test_gpu_matches_oracle_cylinder_200(ib, orc):
+    """The 200x200, 3-level, 157-point cylinder at Re 100, dt 0.004 (the reference's CPU case), 30 steps."""
+    nsteps = 30
+    prob = ib.configs.cylinder_re100_200()
+    sg = ib.State(prob)
+    so = ib.State(prob)
+    gpu = ib.create_solver(sg)
+    cpu = orc.OracleSolver(so)
+    for k in range(nsteps):
+        gpu.advance_()
+        cpu.advance_(pull=False)
+    cpu.pull()
+    gpu.getstate()
+    assert sg.index == so.index == nsteps
+    assert rel_l2(sg.Gamma, so.Gamma) <= TOL_GAMMA
+    assert rel_l2(sg.q, so.q) <= TOL_GAMMA
+    fg, fo = sg.fb.sum(axis=0), so.fb.sum(axis=0)
+    cd_g, cd_o = 2 * fg, 2 * fo  # C = 2F / (U^2 D), U = D = 1
+    assert np.abs(cd_g - cd_o).max() <= TOL_FORCE * max(1.0, np.abs(cd_o).max())
+
+
+def test_gpu_seeded_noise_1024_levels(ib, orc):
+    """Seeded vorticity noise (amplitude 1e-3) on a 128x128, 4-level cylinder, 5 steps."""
+    prob = ib.configs.small_cylinder(128, 4)
+    sg = ib.configs.seed_vorticity(ib.State(prob))
+    so = ib.configs.seed_vorticity(ib.State(prob))
+    gpu = ib.create_solver(sg)
+    cpu = orc.OracleSolver(so)
+    for _ in range(5):
+        gpu.advance_()
+        cpu.advance_(pull=False)
+    cpu.pull()
+    gpu.getstate()
+    assert rel_l2(sg.Gamma, so.Gamma) <= TOL_GAMMA
+    assert np.abs(sg.fb - so.fb).max() <= TOL_FORCE * np.abs(so.fb).max()
+
+
+def test_gpu_time_index_and_solve(ib):
+    # test/solver.jl:61-62
+    prob = ib.configs.small_cylinder(64, 3)
+    st = ib.State(prob)
+    solver = ib.create_solver(st)
+    ib.solve_(solver, t=3 * ib.timestep(prob))
+    assert st.index == 3
+    assert st.t == pytest.approx(2 * ib.timestep(prob))
+
+
+def test_gpu_outside_allowed_region(ib):
+    # test/solver.jl:66-79
+    fluid = ib.Fluid(grid=ib.fluid_grid(h=0.1, xlims=(-1.0, 0.5), ylims=(-1.0, 1.0), nlevel=3), Re=20.0,
+                     freestream_vel=lambda t: (1.0, 0.0))
+    panels = ib.Curves.panels_for(fluid.grid, ib.Curves.Circle(r=0.5, center=(0.0, 0.0)))
+    prob = ib.Problem(fluid=fluid, bodies=ib.Bodies(cyl=ib.StaticBody(panels)),
+                      scheme=ib.default_scheme(fluid.grid, Umax=2.0, cfl=0.2))
+    with pytest.raises(RuntimeError, match="outside allowed region"):
+        ib.create_solver(ib.State(prob))
+
+
+def test_gpu_state_roundtrip_and_resume(ib):
+    """A checkpoint taken after 3 steps resumes to the same state as an uninterrupted run."""
+    prob = ib.configs.small_cylinder(64, 3)
+    a = ib.State(prob)
+    sa = ib.create_solver(a)
+    for _ in range(6):
+        sa.advance_()
+    sa.getstate()
+    b = ib.State(prob)
+    sb = ib.create_solver(b)
+    for _ in range(3):
+        sb.advance_()
+    blob = ib.io.state_bytes(sb.getstate())
+    import io as _io
+
+    c = ib.load_state(_io.BytesIO(blob), prob)
+    sc = ib.create_solver(c)
+    for _ in range(3):
+        sc.advance_()
+    sc.getstate()
+    assert np.array_equal(c.Gamma, a.Gamma)
+    assert np.array_equal(c.q, a.q)
+    assert np.array_equal(c.fb, a.fb)
+
+
+def test_gpu_deterministic(ib):
+    prob = ib.configs.small_cylinder(64, 3)
+    out = []
+    for _ in range(2):
+        st = ib.State(prob)
+        s = ib.create_solver(st)
+        for _ in range(4):
+            s.advance_()
+        s.getstate()
+        out.append((st.Gamma.copy(), st.fb.copy()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
