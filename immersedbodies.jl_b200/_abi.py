@@ -71,6 +71,11 @@ EXPORTS = {
     "ibpm_kernel_launches": (C.c_int64, [C.c_void_p]),
     "ibpm_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "ibpm_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), _dp, _dp]),
+    "ibpm_diag_solve": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp]),
+    "ibpm_diag_apply_B": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "ibpm_diag_binv": (C.c_int, [C.c_void_p, _dp]),
+    "ibpm_diag_vort2flux": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "ibpm_diag_reg": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
 }
 KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3}
 

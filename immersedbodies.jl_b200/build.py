@@ -1,4 +1,9 @@
-"""Builds libibpm_b200.so in-tree for sm_100a (nvcc, no JIT cache)."""
+"""Builds libibpm_b200.so in-tree for sm_100a (nvcc, no JIT cache).
+
+Two translation units: ibpm.cu (transforms, stencils, host runtime and C ABI)
+and coupling.cu, compiled with -fmad=false so the regularised-delta weights
+and the E / E^T sums round exactly like the reference (no fused multiply-add).
+"""
 from __future__ import annotations
 
 import os
@@ -6,25 +11,34 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", "ibpm.cu")]
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "lib", "obj")
 OUT = os.path.join(HERE, "lib", "libibpm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "550"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "550"]
+UNITS = [("ibpm.cu", []), ("coupling.cu", ["-fmad=false"])]
 
 
 def _deps():
-    d = os.path.join(HERE, "csrc")
-    return [os.path.join(d, f) for f in os.listdir(d)] + [os.path.join(HERE, "..", "include", "ibpm_b200.h")]
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "ibpm_b200.h")]
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    os.makedirs(OBJ, exist_ok=True)
     if not force and os.path.exists(OUT):
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(p) <= t for p in _deps()):
             return OUT
-    cmd = [NVCC, *FLAGS, "-o", OUT, *SRC]
+    objs = []
+    for src, extra in UNITS:
+        obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+        cmd = [NVCC, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

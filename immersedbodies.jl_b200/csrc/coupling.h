@@ -1,0 +1,18 @@
+// coupling.h -- launchers of the coupling kernels (coupling.cu, built with -fmad=false).
+#pragma once
+#include "common.cuh"
+
+namespace ibpm {
+
+constexpr int kTile = 16;  // faces per side of a reg! gather tile
+
+void launch_reg_weights(const Panels &P, int p0, int p1, const Grid &g, cudaStream_t st);
+void launch_bbox(const Panels &P, const Grid &g, cudaStream_t st);
+void launch_reg_patch(const Panels &P, const double *f, long long fbs, double *patch, long long pbs, int nbatch,
+                      const Grid &g, cudaStream_t st);
+void launch_regT(const Panels &P, const double *q, long long qbs, double *out, long long obs, int nbatch, int add_q0,
+                 const StepDev *prm, const Grid &g, cudaStream_t st);
+void launch_rigid_motion(const Panels &P, const double *ref_xb, const double *motion, int p0, int p1,
+                         cudaStream_t st);
+
+}  // namespace ibpm

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/ibpm_b200.h"
+#include "coupling.h"
 #include "kernels.cuh"
 
 using namespace ibpm;
@@ -253,9 +254,7 @@ struct ibpm_handle {
 
     // Regularisation patch of nbatch force vectors f (stride 2np).
     void reg_patch(const double *f, int nbatch) {
-        const int tiles_x = (nx + 1 + kTile - 1) / kTile + 1, tiles_y = (ny + 1 + kTile - 1) / kTile + 1;
-        const dim3 grd(tiles_x, tiles_y, nbatch);
-        reg_patch_kernel<<<grd, 256, 0, st>>>(P, f, 2 * np, patch, patch_stride);
+        launch_reg_patch(P, f, 2 * np, patch, patch_stride, nbatch, g, st);
         check_launch();
     }
 
@@ -270,19 +269,18 @@ struct ibpm_handle {
             CK(cudaMemset2DAsync(Gw + ng, (size_t)(ng * L) * sizeof(double), 0, (size_t)(ng * (L - 1)) * sizeof(double),
                                  nbatch, st));
         vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false);
-        const int nt = 2 * np * nbatch;
-        regT_kernel<<<(nt + 127) / 128, 128, 0, st>>>(P, qw, nq, x, xs, nbatch, 0, prm, g);
+        launch_regT(P, qw, nq, x, xs, nbatch, 0, prm, g, st);
         check_launch();
     }
 
     void update_weights(int p0, int p1) {
         if (p1 <= p0) return;
-        reg_weights_kernel<<<p1 - p0, dim3(49, 2), 0, st>>>(P, p0, g);
+        launch_reg_weights(P, p0, p1, g, st);
         check_launch();
     }
 
     void compute_bbox() {
-        bbox_kernel<<<1, 256, 0, st>>>(P, g);
+        launch_bbox(P, g, st);
         check_launch();
     }
 
@@ -549,7 +547,7 @@ void ibpm_handle::step(const ibpm_step_params &sp) {
         for (int b = 0; b < nbody; ++b) {
             if (body_kind[b] != IBPM_BODY_MOVING_RIGID) continue;
             const int p0 = body_start[b], p1 = body_start[b + 1];
-            rigid_motion_kernel<<<(p1 - p0 + 127) / 128, 128, 0, st>>>(P, ref_xb_d, motion + 6 * b, p0, p1);
+            launch_rigid_motion(P, ref_xb_d, motion + 6 * b, p0, p1, st);
             check_launch();
             update_weights(p0, p1);
         }
@@ -580,8 +578,7 @@ void ibpm_handle::step(const ibpm_step_params &sp) {
     vort2flux(psi, qs1, Gnew, 0, 0, 1, false);
     // couple_surface_rigid (src/coupling.jl:236-250)
     {
-        const int nt = 2 * np;
-        regT_kernel<<<(nt + 127) / 128, 128, 0, st>>>(P, qs1, 0, Ftmp, 0, 1, 1, prm, g);
+        launch_regT(P, qs1, 0, Ftmp, 0, 1, 1, prm, g, st);
         check_launch();
     }
     const int n = 2 * np;
@@ -608,6 +605,14 @@ void ibpm_handle::step(const ibpm_step_params &sp) {
 }
 
 namespace {
+// Evaluates an X-pass prologue functor on every (i, j) of one field (diagnostics).
+template <class In>
+__global__ void eval_prologue_kernel(In in, double *out, int nx, int ny) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > nx - 1 || j > ny - 1) return;
+    out[(long long)(i - 1) + (long long)(nx - 1) * (j - 1)] = in(0, i, j);
+}
+
 __global__ void q0_fill_kernel(double *q0, const StepDev *prm, Grid g) {
     const long long nu = (long long)(g.nx + 1) * g.ny, nq = nu + (long long)g.nx * (g.ny + 1);
     const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -720,6 +725,22 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
             return IBPM_ERR_INVALID;
         }
         if (h->body_kind[b] != IBPM_BODY_STATIC) h->static_bodies = false;
+    }
+    // The reference rejects out-of-region static panels while building the
+    // Regularization (coupling.jl:38-41), before any size restriction of ours.
+    for (int b = 0; b < p->nbody; ++b) {
+        if (h->body_kind[b] != IBPM_BODY_STATIC) continue;
+        for (int k = h->body_start[b]; k < h->body_start[b + 1]; ++k) {
+            const double xb = h->ref_xb[k], yb = h->ref_xb[p->npanel + k];
+            const int ix = (int)nearbyint((xb - p->x0) / p->h + 1.0 - 0.25);
+            const int iy = (int)nearbyint((yb - p->y0) / p->h + 1.0 - 0.25);
+            if (!(3 < ix && ix <= p->nx - 3) || !(3 < iy && iy <= p->ny - 3)) {
+                g_create_error = "Panel index=" + std::to_string(k + 1) + " at (" + ibpm_handle::jl_float(xb) + ", " +
+                                 ibpm_handle::jl_float(yb) + ") outside allowed region";
+                delete h;
+                return IBPM_ERR_REGION;
+            }
+        }
     }
     const int rc = guarded(h, [&] { h->setup(); });
     if (rc != IBPM_OK) {
@@ -844,6 +865,88 @@ const char *ibpm_last_error(const ibpm_handle *h) { return h ? h->last_error.c_s
 void *ibpm_stream(ibpm_handle *h) { return h ? (void *)h->st : nullptr; }
 
 int64_t ibpm_kernel_launches(const ibpm_handle *h) { return h ? h->launches : 0; }
+
+int ibpm_diag_solve(ibpm_handle *h, int op, int level, const double *b, double *x) {
+    if (!h || !b || !x || op < 0 || op > 2 || level < 1 || level > h->L) return IBPM_ERR_INVALID;
+    return guarded(h, [&] {
+        CK(cudaSetDevice(h->device));
+        const size_t bytes = sizeof(double) * h->ng;
+        CK(cudaMemcpyAsync(h->rhs, b, bytes, cudaMemcpyHostToDevice, h->st));
+        const int mode = op == 0 ? MULT_LAPINV : (op == 1 ? MULT_AEXPL : MULT_AIMPL);
+        h->xpass(h->in_plain(h->rhs, h->ng), h->out_plain(h->t1, h->ng), 1);
+        h->ypass(h->t1, h->t2, h->ng, 1, h->mult(mode, level, 0));
+        h->xpass(h->in_plain(h->t2, h->ng), h->out_plain(h->rhs, h->ng), 1);
+        CK(cudaMemcpyAsync(x, h->rhs, bytes, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    });
+}
+
+int ibpm_diag_apply_B(ibpm_handle *h, const double *z, double *x) {
+    if (!h || !z || !x) return IBPM_ERR_INVALID;
+    return guarded(h, [&] {
+        CK(cudaSetDevice(h->device));
+        const size_t bytes = sizeof(double) * 2 * h->np;
+        CK(cudaMemcpyAsync(h->cg_u, z, bytes, cudaMemcpyHostToDevice, h->st));
+        h->compute_bbox();
+        h->apply_B(h->cg_u, h->cg_c, 2 * h->np, 1);
+        CK(cudaMemcpyAsync(x, h->cg_c, bytes, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    });
+}
+
+int ibpm_diag_binv(ibpm_handle *h, double *out) {
+    if (!h || !out) return IBPM_ERR_INVALID;
+    if (!h->Binv) {
+        h->last_error = "no precomputed B^-1 (moving bodies)";
+        return IBPM_ERR_INVALID;
+    }
+    return guarded(h, [&] {
+        const size_t n = 2 * (size_t)h->np;
+        CK(cudaMemcpyAsync(out, h->Binv, sizeof(double) * n * n, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    });
+}
+
+int ibpm_diag_vort2flux(ibpm_handle *h, double *gamma, double *psi, double *q) {
+    if (!h || !gamma || !psi || !q) return IBPM_ERR_INVALID;
+    return guarded(h, [&] {
+        CK(cudaSetDevice(h->device));
+        const size_t ngL = sizeof(double) * h->ng * h->L;
+        CK(cudaMemcpyAsync(h->Gw, gamma, ngL, cudaMemcpyHostToDevice, h->st));
+        double *qd = h->dalloc<double>(h->nq * h->L);
+        h->vort2flux(h->psiw, qd, h->Gw, 0, 0, 1, true);
+        CK(cudaMemcpyAsync(gamma, h->Gw, ngL, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaMemcpyAsync(psi, h->psiw, ngL, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaMemcpyAsync(q, qd, sizeof(double) * h->nq * h->L, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    });
+}
+
+int ibpm_diag_reg(ibpm_handle *h, const double *f, double *gamma1, const double *q1, double *fout) {
+    if (!h) return IBPM_ERR_INVALID;
+    return guarded(h, [&] {
+        CK(cudaSetDevice(h->device));
+        const size_t nf = sizeof(double) * 2 * h->np;
+        h->compute_bbox();
+        if (f && gamma1) {
+            CK(cudaMemcpyAsync(h->cg_u, f, nf, cudaMemcpyHostToDevice, h->st));
+            h->reg_patch(h->cg_u, 1);
+            // the X-pass prologue (InRegRot) evaluated on every Gamma point
+            const dim3 blk(32, 8), grd((h->nx - 1 + 31) / 32, (h->ny - 1 + 7) / 8);
+            eval_prologue_kernel<<<grd, blk, 0, h->st>>>(InRegRot{Patch{h->patch, h->P.bbox, h->patch_stride}}, h->t2,
+                                                         h->nx, h->ny);
+            h->check_launch();
+            CK(cudaMemcpyAsync(gamma1, h->t2, sizeof(double) * h->ng, cudaMemcpyDeviceToHost, h->st));
+        }
+        if (q1 && fout) {
+            CK(cudaMemcpyAsync(h->qw, q1, sizeof(double) * h->nq, cudaMemcpyHostToDevice, h->st));
+            launch_regT(h->P, h->qw, 0, h->cg_c, 0, 1, 0, h->prm, h->g, h->st);
+            h->check_launch();
+            CK(cudaMemcpyAsync(fout, h->cg_c, nf, cudaMemcpyDeviceToHost, h->st));
+        }
+        CK(cudaStreamSynchronize(h->st));
+    });
+}
 
 int ibpm_profile(ibpm_handle *h, int enable) {
     if (!h) return IBPM_ERR_INVALID;

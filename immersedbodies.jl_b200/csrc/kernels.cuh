@@ -1,97 +1,10 @@
-// kernels.cuh -- FP64 device kernels of the IBPM time step.
-//
-// Index helpers use the reference's 1-based (i, j) so each kernel reads like
-// the loop it restates.  Layouts (column-major, x fastest):
-//   Gamma-like field  (nx-1) x (ny-1):  GI(i,j) = (i-1) + (nx-1)(j-1)
-//   x flux  (nx+1) x ny:                UI(i,j) = (i-1) + (nx+1)(j-1)
-//   y flux  nx x (ny+1):                VI(i,j) = nu + (i-1) + nx(j-1)
-// A "batch" index b selects a field: either the level (b = lev-1, the trial
-// solves) or an independent right-hand side (the B^-1 setup columns).
+// kernels.cuh -- FP64 device kernels of the IBPM time step (line passes,
+// stencils, B^-1 algebra).  Included by ibpm.cu only.
 #pragma once
+#include "common.cuh"
 #include "fft_dst.cuh"
 
 namespace ibpm {
-
-struct Grid {
-    int nx, ny, L;
-    double h, x0, y0, Re, dt;
-    int grid_moving;
-};
-
-// Per-step host-callback values, resident in device memory.
-struct StepDev {
-    double fs[2];   // freestream velocity
-    double gm[6];   // grid motion: center(2), vel(2), angle, angular_vel
-};
-
-#define GI(i, j) ((long long)((i)-1) + (long long)(g.nx - 1) * (long long)((j)-1))
-#define UI(i, j) ((long long)((i)-1) + (long long)(g.nx + 1) * (long long)((j)-1))
-#define VI(i, j) (nu + (long long)((i)-1) + (long long)g.nx * (long long)((j)-1))
-
-enum { SIDE_B = 0, SIDE_T = 1, SIDE_L = 2, SIDE_R = 3 };
-
-__device__ __forceinline__ double gridstep(const Grid &g, int lev) { return ldexp(g.h, lev - 1); }
-
-// get_bc! (src/fluid.jl:278-306), one entry: rbc[side offset + ibc] from the
-// coarser level's field r.  r == nullptr means zero boundary values.
-__device__ __forceinline__ double getbc(const double *__restrict__ r, const Grid &g, int side, int ibc) {
-    if (r == nullptr) return 0.0;
-    const int nx = g.nx, ny = g.ny;
-    if (side == SIDE_B || side == SIDE_T) {
-        const int row = side == SIDE_B ? ny / 4 : 3 * ny / 4;
-        if (ibc & 1) return r[GI(nx / 4 + (ibc - 1) / 2, row)];
-        const int i = nx / 4 + ibc / 2;
-        return 0.5 * (r[GI(i, row)] + r[GI(i - 1, row)]);
-    }
-    const int col = side == SIDE_L ? nx / 4 : 3 * nx / 4;
-    if (ibc & 1) return r[GI(col, ny / 4 + (ibc - 1) / 2)];
-    const int j = ny / 4 + ibc / 2;
-    return 0.5 * (r[GI(col, j)] + r[GI(col, j - 1)]);
-}
-
-// apply_bc! contribution at (i, j) (src/fluid.jl:308-338), accumulated in the
-// reference's order (bottom/top rows first, then left/right columns).
-__device__ __forceinline__ double apply_bc_at(double v, const double *__restrict__ r, const Grid &g, int i, int j,
-                                              double fac) {
-    if (j == 1) v += fac * getbc(r, g, SIDE_B, i + 1);
-    if (j == g.ny - 1) v += fac * getbc(r, g, SIDE_T, i + 1);
-    if (i == 1) v += fac * getbc(r, g, SIDE_L, j + 1);
-    if (i == g.nx - 1) v += fac * getbc(r, g, SIDE_R, j + 1);
-    return v;
-}
-
-__device__ __forceinline__ bool on_ring(const Grid &g, int i, int j) {
-    return j == 1 || j == g.ny - 1 || i == 1 || i == g.nx - 1;
-}
-
-// base_flux! (src/fluid.jl:22-67), evaluated per face instead of stored.
-__device__ __forceinline__ double base_flux_x(const Grid &g, const StepDev *__restrict__ prm, int lev, int i, int j) {
-    const double hc = gridstep(g, lev);
-    if (!g.grid_moving) return prm->fs[0] * hc;
-    const double cx = prm->gm[0], cy = prm->gm[1], th = prm->gm[4], Om = prm->gm[5];
-    double st, ct;
-    sincos(th, &st, &ct);
-    const double x0 = g.x0 + g.nx * (g.h - hc) / 2, y0 = g.y0 + g.ny * (g.h - hc) / 2;
-    const double x = x0 + hc * (i - 1), y = y0 + hc / 2 + hc * (j - 1);
-    const double dx = x - cx, dy = y - cy;
-    const double wx = prm->fs[0] - prm->gm[2] - ((Om * -st) * dx + (Om * -ct) * dy);
-    const double wy = prm->fs[1] - prm->gm[3] - ((Om * ct) * dx + (Om * -st) * dy);
-    return hc * (ct * wx + st * wy);
-}
-
-__device__ __forceinline__ double base_flux_y(const Grid &g, const StepDev *__restrict__ prm, int lev, int i, int j) {
-    const double hc = gridstep(g, lev);
-    if (!g.grid_moving) return prm->fs[1] * hc;
-    const double cx = prm->gm[0], cy = prm->gm[1], th = prm->gm[4], Om = prm->gm[5];
-    double st, ct;
-    sincos(th, &st, &ct);
-    const double x0 = g.x0 + g.nx * (g.h - hc) / 2, y0 = g.y0 + g.ny * (g.h - hc) / 2;
-    const double x = x0 + hc / 2 + hc * (i - 1), y = y0 + hc * (j - 1);
-    const double dx = x - cx, dy = y - cy;
-    const double wx = prm->fs[0] - prm->gm[2] - ((Om * -st) * dx + (Om * -ct) * dy);
-    const double wy = prm->fs[1] - prm->gm[3] - ((Om * ct) * dx + (Om * -st) * dy);
-    return hc * (-st * wx + ct * wy);
-}
 
 // ---------------------------------------------------------------------------
 // Line-pass kernels
@@ -119,20 +32,6 @@ struct InBC {
         double v = G[GI(i, j)];
         if (on_ring(g, i, j)) v = apply_bc_at(v, coarse + b * cbs, g, i, j, 1.0);
         return v;
-    }
-};
-
-// Regularised flux on the panels' bounding box (compact patch):
-// patch[(i - i0) + pw (j - j0)] for x faces, offset pw*ph for y faces.
-struct Patch {
-    const double *p;
-    const int *bbox;      // device: i0, i1, j0, j1 (1-based face indices)
-    long long bs;
-    __device__ __forceinline__ double get(int b, int comp, int i, int j) const {
-        const int i0 = bbox[0], i1 = bbox[1], j0 = bbox[2], j1 = bbox[3];
-        if (i < i0 || i > i1 || j < j0 || j > j1) return 0.0;
-        const int pw = i1 - i0 + 1, ph = j1 - j0 + 1;
-        return p[b * bs + (long long)comp * pw * ph + (i - i0) + (long long)pw * (j - j0)];
     }
 };
 
@@ -404,211 +303,6 @@ __global__ void coarsify_kernel(double *__restrict__ coarse, const double *__res
                      0.25 * (G[GI(i + 1, j + 1)] + G[GI(i + 1, j - 1)] + G[GI(i - 1, j - 1)] + G[GI(i - 1, j + 1)]);
 }
 
-// ---------------------------------------------------------------------------
-// Coupling kernels (src/coupling.jl)
-// ---------------------------------------------------------------------------
-
-// Yang3 smoothed delta times h (src/coupling.jl:91-148), the published
-// polynomial of Yang et al., JCP 2009, with the reference's constants.
-__device__ __forceinline__ double delta_h(double rf, double rb, double dr) {
-    const double r = fabs(rf - rb);
-    const double r1 = r / dr;
-    const double r2 = r1 * r1;
-    const double r3 = r2 * r1;
-    const double r4 = r3 * r1;
-    if (r1 <= 1.0) {
-        const double a5 = asin((1.0 / 2.0) * sqrt(3.0) * (2.0 * r1 - 1.0));
-        const double a8 = sqrt(1.0 - 12.0 * r2 + 12.0 * r1);
-        return 4.166666667e-2 * r4 + (-0.1388888889 + 3.472222222e-2 * a8) * r3 +
-               (-7.121664902e-2 - 5.208333333e-2 * a8 + 0.2405626122 * a5) * r2 +
-               (-0.2405626122 * a5 - 0.3792313933 + 0.1012731481 * a8) * r1 + 8.0187537413e-2 * a5 -
-               4.195601852e-2 * a8 + 0.6485698427;
-    } else if (r1 <= 2.0) {
-        const double a6 = asin((1.0 / 2.0) * sqrt(3.0) * (-3.0 + 2.0 * r1));
-        const double a9 = sqrt(-23.0 + 36.0 * r1 - 12.0 * r2);
-        return -6.250000000e-2 * r4 + (0.4861111111 - 1.736111111e-2 * a9) * r3 +
-               (-1.143175026 + 7.812500000e-2 * a9 - 0.1202813061 * a6) * r2 +
-               (0.8751991178 + 0.3608439183 * a6 - 0.1548032407 * a9) * r1 - 0.2806563809 * a6 + 8.22848104e-3 +
-               0.1150173611 * a9;
-    } else if (r1 <= 3.0) {
-        const double a1 = asin((1.0 / 2.0 * (2.0 * r1 - 5.0)) * sqrt(3.0));
-        const double a7 = sqrt(-71.0 - 12.0 * r2 + 60.0 * r1);
-        return 2.083333333e-2 * r4 + (3.472222222e-3 * a7 - 0.2638888889) * r3 +
-               (1.214391675 - 2.604166667e-2 * a7 + 2.405626122e-2 * a1) * r2 +
-               (-0.1202813061 * a1 - 2.449273192 + 7.262731481e-2 * a7) * r1 + 0.1523563211 * a1 + 1.843201677 -
-               7.306134259e-2 * a7;
-    }
-    return 0.0;
-}
-
-struct Panels {
-    int np;
-    double *xb;        // np x 2 (current positions)
-    double *ub;        // np x 2
-    int *pc;           // np x 2 panel_coords (ix, iy)
-    double *w;         // np x 2 x 49, [(p*2+c)*49 + bb*7 + a]
-    int *bbox;         // i0, i1, j0, j1 of the support union (face indices)
-    int *err;          // err[0]: 0 or 1-based panel index outside the region
-};
-
-// _update!(reg, index, point) (src/coupling.jl:27-54) for panels [p0, p1).
-// One block of 49 x 2 threads per panel.
-__global__ void reg_weights_kernel(Panels P, int p0, Grid g) {
-    const int p = p0 + blockIdx.x;
-    const int a = threadIdx.x % 7, bb = threadIdx.x / 7, c = threadIdx.y;
-    const double h = g.h, x0 = g.x0, y0 = g.y0;
-    const double xb = P.xb[p], yb = P.xb[P.np + p];
-    const int ix = (int)rint((xb - x0) / h + 1.0 - 0.25);
-    const int iy = (int)rint((yb - y0) / h + 1.0 - 0.25);
-    const bool ok = (3 < ix && ix <= g.nx - 3) && (3 < iy && iy <= g.ny - 3);
-    if (!ok) {
-        if (threadIdx.x == 0 && threadIdx.y == 0) atomicCAS(P.err, 0, p + 1);
-        return;
-    }
-    if (threadIdx.x == 0 && c == 0) {
-        P.pc[2 * p] = ix;
-        P.pc[2 * p + 1] = iy;
-    }
-    const double x = x0 + h * ((ix + (a - 3)) - 1);
-    const double y = y0 + h * ((iy + (bb - 3)) - 1);
-    double wv;
-    if (c == 0)
-        wv = delta_h(x, xb, h) * delta_h(y + h / 2, yb, h);
-    else
-        wv = delta_h(x + h / 2, xb, h) * delta_h(y, yb, h);
-    P.w[(long long)(p * 2 + c) * 49 + bb * 7 + a] = wv;
-}
-
-// Union of the panels' 7x7 supports (one block).
-__global__ void bbox_kernel(Panels P, Grid g) {
-    __shared__ int s[4][32];
-    int i0 = 1 << 30, i1 = -(1 << 30), j0 = 1 << 30, j1 = -(1 << 30);
-    for (int p = threadIdx.x; p < P.np; p += blockDim.x) {
-        const int ix = P.pc[2 * p], iy = P.pc[2 * p + 1];
-        i0 = min(i0, ix - 3);
-        i1 = max(i1, ix + 3);
-        j0 = min(j0, iy - 3);
-        j1 = max(j1, iy + 3);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        i0 = min(i0, __shfl_xor_sync(0xffffffffu, i0, o));
-        i1 = max(i1, __shfl_xor_sync(0xffffffffu, i1, o));
-        j0 = min(j0, __shfl_xor_sync(0xffffffffu, j0, o));
-        j1 = max(j1, __shfl_xor_sync(0xffffffffu, j1, o));
-    }
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        s[0][w] = i0;
-        s[1][w] = i1;
-        s[2][w] = j0;
-        s[3][w] = j1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
-            i0 = min(i0, s[0][k]);
-            i1 = max(i1, s[1][k]);
-            j0 = min(j0, s[2][k]);
-            j1 = max(j1, s[3][k]);
-        }
-        P.bbox[0] = max(i0, 1);
-        P.bbox[1] = i1;
-        P.bbox[2] = max(j0, 1);
-        P.bbox[3] = j1;
-    }
-}
-
-// reg! (src/coupling.jl:72-85) as a deterministic gather over a 16x16 tile of
-// faces: the block lists, in panel order, the panels whose support meets the
-// tile, then every face sums w * f over that list in panel order -- the same
-// accumulation order as the reference's sequential loop over panels.
-// f: 2np per batch (x block then y block); patch output per batch.
-constexpr int kTile = 16;
-__global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *__restrict__ f, long long fbs,
-                                                        double *__restrict__ patch, long long pbs) {
-    __shared__ int list[1024];
-    __shared__ int warp_cnt[8];
-    __shared__ int total;
-    const int i0 = P.bbox[0], i1 = P.bbox[1], j0 = P.bbox[2], j1 = P.bbox[3];
-    const int pw = i1 - i0 + 1, ph = j1 - j0 + 1;
-    const int ti0 = i0 + blockIdx.x * kTile, tj0 = j0 + blockIdx.y * kTile;
-    if (ti0 > i1 || tj0 > j1) return;
-    const int ti1 = min(ti0 + kTile - 1, i1), tj1 = min(tj0 + kTile - 1, j1);
-    const int b = blockIdx.z;
-    const double *fb = f + b * fbs;
-    double *out = patch + b * pbs;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int li = tid % kTile, lj = tid / kTile;
-    const int i = ti0 + li, j = tj0 + lj;
-    double accx = 0.0, accy = 0.0;
-    int base = 0;
-    for (int c0 = 0; c0 < P.np; c0 += 256) {
-        if (tid == 0) total = 0;
-        const int p = c0 + tid;
-        bool hit = false;
-        if (p < P.np) {
-            const int ix = P.pc[2 * p], iy = P.pc[2 * p + 1];
-            hit = ix + 3 >= ti0 && ix - 3 <= ti1 && iy + 3 >= tj0 && iy - 3 <= tj1;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (lane == 0) warp_cnt[w] = __popc(m);
-        __syncthreads();
-        int off = 0;
-        for (int k = 0; k < w; ++k) off += warp_cnt[k];
-        if (hit) list[off + __popc(m & ((1u << lane) - 1))] = p;
-        if (tid == 255) {
-            int s = 0;
-            for (int k = 0; k < 8; ++k) s += warp_cnt[k];
-            total = s;
-        }
-        __syncthreads();
-        (void)base;
-        const int n = total;
-        if (i <= ti1 && j <= tj1) {
-            for (int k = 0; k < n; ++k) {
-                const int q = list[k];
-                const int ix = P.pc[2 * q], iy = P.pc[2 * q + 1];
-                const int da = i - ix + 3, db = j - iy + 3;
-                if (da >= 0 && da < 7 && db >= 0 && db < 7) {
-                    accx = accx + P.w[(long long)(q * 2) * 49 + db * 7 + da] * fb[q];
-                    accy = accy + P.w[(long long)(q * 2 + 1) * 49 + db * 7 + da] * fb[P.np + q];
-                }
-            }
-        }
-        __syncthreads();
-    }
-    if (i <= ti1 && j <= tj1) {
-        out[(i - i0) + (long long)pw * (j - j0)] = accx;
-        out[(long long)pw * ph + (i - i0) + (long long)pw * (j - j0)] = accy;
-    }
-}
-
-// regT! (src/coupling.jl:57-69): fb[p, c] = dot(q_c[7x7 at p], w[p, c]) in
-// column-major order.  With add_q0 it is couple_surface_rigid's
-// Ftmp = E (qs + q0) - ub h (src/coupling.jl:239-244).
-__global__ void regT_kernel(Panels P, const double *__restrict__ q, long long qbs, double *__restrict__ out,
-                            long long obs, int nbatch, int add_q0, const StepDev *__restrict__ prm, Grid g) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int np = P.np;
-    if (t >= 2 * np * nbatch) return;
-    const int b = t / (2 * np), pcomp = t % (2 * np);
-    const int c = pcomp / np, p = pcomp % np;
-    const long long nu = (long long)(g.nx + 1) * g.ny;
-    const double *Q = q + b * qbs;
-    const int i0 = P.pc[2 * p] - 3, j0 = P.pc[2 * p + 1] - 3;
-    const double *w = P.w + (long long)(p * 2 + c) * 49;
-    double s = 0.0;
-    for (int bb = 0; bb < 7; ++bb)
-        for (int a = 0; a < 7; ++a) {
-            const int i = i0 + a, j = j0 + bb;
-            double v = c == 0 ? Q[UI(i, j)] : Q[VI(i, j)];
-            if (add_q0) v = v + (c == 0 ? base_flux_x(g, prm, 1, i, j) : base_flux_y(g, prm, 1, i, j));
-            s += v * w[bb * 7 + a];
-        }
-    if (add_q0) s = s - P.ub[c * np + p] * g.h;
-    out[b * obs + c * np + p] = s;
-}
-
 // x = Binv z for the precomputed B^-1 (src/coupling.jl:187-192), column-major n x n.
 // Grid (ceil(n/64), ceil(n/64)); partial sums part[chunk * n + row], summed in
 // chunk order by binv_reduce_kernel (deterministic).
@@ -669,22 +363,6 @@ __global__ void binv_reduce_kernel(const double *__restrict__ part, int nchunk, 
         total[0] = ax;
         total[1] = ay;
     }
-}
-
-// _update!(panels, ::MovingRigidBody, t) (src/bodies.jl:12-31) for panels [p0, p1)
-// with motion m = pos(2), vel(2), angle, angular_vel.
-__global__ void rigid_motion_kernel(Panels P, const double *__restrict__ ref_xb, const double *__restrict__ motion,
-                                    int p0, int p1) {
-    const int p = p0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= p1) return;
-    const double r0x = motion[0], r0y = motion[1], v0x = motion[2], v0y = motion[3], ang = motion[4], Om = motion[5];
-    double sn, c;
-    sincos(ang, &sn, &c);
-    const double rx = ref_xb[p], ry = ref_xb[P.np + p];
-    P.xb[p] = r0x + (c * rx + -sn * ry);
-    P.xb[P.np + p] = r0y + (sn * rx + c * ry);
-    P.ub[p] = v0x + ((Om * -sn) * rx + (Om * -c) * ry);
-    P.ub[P.np + p] = v0y + ((Om * c) * rx + (Om * -sn) * ry);
 }
 
 // In-place Gauss-Jordan inversion of a symmetric positive definite matrix

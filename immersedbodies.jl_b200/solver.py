@@ -166,6 +166,46 @@ class GpuCnabSolver(AbstractSolver):
                                                                   C.byref(ms), C.byref(b)))
         return n.value, ms.value, b.value
 
+    def diag_solve(self, op: int, level: int, b: np.ndarray) -> np.ndarray:
+        """One DST-diagonalised solve on the device: op 0 Δinv, 1 A, 2 Ainv (at `level`)."""
+        b = np.asfortranarray(b, dtype=np.float64)
+        x = np.empty_like(b, order="F")
+        _abi.check(self.lib, self._h, self.lib.ibpm_diag_solve(self._h, op, level, _abi.dptr(b), _abi.dptr(x)))
+        return x
+
+    def diag_apply_B(self, z: np.ndarray) -> np.ndarray:
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        x = np.empty_like(z)
+        _abi.check(self.lib, self._h, self.lib.ibpm_diag_apply_B(self._h, _abi.dptr(z), _abi.dptr(x)))
+        return x
+
+    def diag_binv(self) -> np.ndarray:
+        n = 2 * self.state.prob.bodies.npanel
+        out = np.empty((n, n), order="F")
+        _abi.check(self.lib, self._h, self.lib.ibpm_diag_binv(self._h, _abi.dptr(out)))
+        return out
+
+    def diag_vort2flux(self, gamma: np.ndarray):
+        """vort2flux on the device: returns (coarsified gamma, psi, q)."""
+        g = np.asfortranarray(gamma, dtype=np.float64).copy(order="F")
+        psi = np.zeros_like(g, order="F")
+        q = np.zeros((self.state.q.shape[0], g.shape[1]), order="F")
+        _abi.check(self.lib, self._h, self.lib.ibpm_diag_vort2flux(self._h, _abi.dptr(g), _abi.dptr(psi),
+                                                                    _abi.dptr(q)))
+        return g, psi, q
+
+    def diag_reg_rot(self, f: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.zeros(self.state.Gamma.shape[0])
+        _abi.check(self.lib, self._h, self.lib.ibpm_diag_reg(self._h, _abi.dptr(f), _abi.dptr(out), None, None))
+        return out
+
+    def diag_regT(self, q1: np.ndarray) -> np.ndarray:
+        q1 = np.ascontiguousarray(q1, dtype=np.float64)
+        out = np.zeros(2 * self.state.prob.bodies.npanel)
+        _abi.check(self.lib, self._h, self.lib.ibpm_diag_reg(self._h, None, None, _abi.dptr(q1), _abi.dptr(out)))
+        return out
+
     def advance_many(self, nsteps: int):
         """nsteps advance! calls in one library call (params evaluated on the host
         up front); the host State's index/t/fb are updated at the end."""

@@ -153,6 +153,23 @@ int64_t ibpm_kernel_launches(const ibpm_handle *h);
 int ibpm_profile(ibpm_handle *h, int enable);
 int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms, double *bytes);
 
+/* Diagnostics: single operators of the step on caller host buffers, for
+ * operator-level parity tests.
+ *   ibpm_diag_solve: x = S(S(b) scale / Lambda) on one (nx-1) x (ny-1) field with
+ *     op 0: Lambda = lap_eigs (Δinv_operator, fluid.jl:117-119),
+ *     op 1: A at `level`, op 2: Ainv at `level` (A_operator, fluid.jl:121-134).
+ *   ibpm_diag_apply_B: x = B z (B_operator, coupling.jl:163-176), 2*npanel.
+ *   ibpm_diag_binv: the precomputed B^-1 (2np x 2np, column-major); static bodies only. */
+int ibpm_diag_solve(ibpm_handle *h, int op, int level, const double *b, double *x);
+int ibpm_diag_apply_B(ibpm_handle *h, const double *z, double *x);
+int ibpm_diag_binv(ibpm_handle *h, double *out);
+/* vort2flux (fluid.jl:178-205) on host buffers: gamma (ng x L) is coarsified in
+ * place (as in the reference), psi (ng x L) and q (nq x L) are outputs. */
+int ibpm_diag_vort2flux(ibpm_handle *h, double *gamma, double *psi, double *q);
+/* rot!(reg!(f)) (fluid.jl:101-111 after coupling.jl:72-85) into gamma1 (ng), and
+ * regT!(f, q1) (coupling.jl:57-69) from a level-1 flux q1 (nq); NULL skips either. */
+int ibpm_diag_reg(ibpm_handle *h, const double *f, double *gamma1, const double *q1, double *fout);
+
 #ifdef __cplusplus
 }
 #endif

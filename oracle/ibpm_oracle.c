@@ -889,6 +889,13 @@ static void project_circ(orc_solver *s) {
     for (size_t k = 0; k < ng; k++) s->G[k] -= s->Gs[k];
 }
 
+void orc_reg_rot(orc_solver *s, const double *f, double *gamma1) {
+    reg(s, s->qtmp2, f);
+    rot(s, gamma1, s->qtmp2);
+}
+
+void orc_regT(orc_solver *s, const double *q1, double *f) { regT(s, f, q1); }
+
 void orc_update_vars(orc_solver *s) {
     const double dt = s->p.dt, h = s->p.h;
     for (int k = 0; k < 2 * s->np; k++) s->fb[k] = s->Fbt[k] * h / dt;

@@ -93,6 +93,9 @@ int orc_binv(orc_solver *s, double *out);
 void orc_apply_B(orc_solver *s, double *x, const double *z);
 /* vort2flux! on caller arrays (src/fluid.jl:175-206); Gamma is coarsified in place. */
 void orc_vort2flux(orc_solver *s, double *psi, double *q, double *gamma);
+/* rot!(Gamma, reg!(q, f)) (fluid.jl:101-111, coupling.jl:72-85) and regT! (coupling.jl:57-69) */
+void orc_reg_rot(orc_solver *s, const double *f, double *gamma1);
+void orc_regT(orc_solver *s, const double *q1, double *f);
 /* update_vars! (src/problem.jl:676-685) */
 void orc_update_vars(orc_solver *s);
 

@@ -73,6 +73,8 @@ def load():
     lib.orc_binv.argtypes = [C.c_void_p, _dp]
     lib.orc_apply_B.argtypes = [C.c_void_p, _dp, _dp]
     lib.orc_vort2flux.argtypes = [C.c_void_p, _dp, _dp, _dp]
+    lib.orc_reg_rot.argtypes = [C.c_void_p, _dp, _dp]
+    lib.orc_regT.argtypes = [C.c_void_p, _dp, _dp]
     lib.orc_nthreads.restype = C.c_int
     lib.orc_nthreads.argtypes = [C.c_int]
     lib.orc_dst1.argtypes = [C.c_int, _dp, _dp]
@@ -263,6 +265,26 @@ class OracleSolver:
         x = np.empty_like(z)
         self.lib.orc_apply_B(self._h, _p(x), _p(z))
         return x
+
+    def vort2flux(self, gamma):
+        """vort2flux! on a copy of gamma (ng x L): returns (coarsified gamma, psi, q)."""
+        g = np.asfortranarray(gamma, dtype=np.float64).copy(order="F")
+        psi = np.zeros_like(g, order="F")
+        q = np.zeros((self.state.q.shape[0], g.shape[1]), order="F")
+        self.lib.orc_vort2flux(self._h, _p(psi), _p(q), _p(g))
+        return g, psi, q
+
+    def reg_rot(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.zeros(self.state.Gamma.shape[0])
+        self.lib.orc_reg_rot(self._h, _p(f), _p(out))
+        return out
+
+    def regT(self, q1):
+        q1 = np.ascontiguousarray(q1, dtype=np.float64)
+        out = np.zeros(2 * self.state.prob.bodies.npanel)
+        self.lib.orc_regT(self._h, _p(q1), _p(out))
+        return out
 
     def total_force(self):
         return self.state.fb.sum(axis=0)

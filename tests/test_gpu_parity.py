@@ -84,8 +84,9 @@ def test_gpu_time_index_and_solve(ib):
     st = ib.State(prob)
     solver = ib.create_solver(st)
     ib.solve_(solver, t=3 * ib.timestep(prob))
-    assert st.index == 3
-    assert st.t == pytest.approx(2 * ib.timestep(prob))
+    # State starts at t0 - dt, so solve! to t = 3 dt takes 4 steps (solver.jl:43)
+    assert st.index == 4
+    assert st.t == pytest.approx(3 * ib.timestep(prob))
 
 
 def test_gpu_outside_allowed_region(ib):
