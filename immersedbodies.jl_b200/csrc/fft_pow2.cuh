@@ -1,0 +1,315 @@
+// fft_pow2.cuh -- DST-I line transform for power-of-two lengths M = 64..1024.
+//
+// Same algorithm as fft_dst.cuh (complex M-point FFT of two packed lines with
+// the sin pre-twiddle and the prefix-scan post-processing), specialised at
+// compile time: the Stockham stages use radix 16 / 8 / 4 butterflies held in
+// registers (three shared-memory round trips for M = 1024 instead of five), all
+// strides and index splits are constants, the shared buffer is padded by one
+// complex per 16 to keep the strided Stockham writes free of bank conflicts,
+// and the post-processing scan runs on warp shuffles with one block barrier.
+#pragma once
+#include "fft_dst.cuh"
+
+namespace ibpm {
+
+// Padded shared-memory index: one spare double2 per 16.
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded_len(int M) { return (M + 1) + ((M + 1) >> 4) + 1; }
+
+// ---- small DFTs (forward, e^{-2 pi i / R}) with constant twiddles ----
+
+constexpr double kR2 = 0.70710678118654752440;   // sqrt(2)/2
+constexpr double kC16 = 0.92387953251128675613;  // cos(pi/8)
+constexpr double kS16 = 0.38268343236508977173;  // sin(pi/8)
+
+// multiply by W16^m for the exponents the radix-16 butterfly needs
+template <int m>
+__device__ __forceinline__ double2 w16(double2 a);
+template <>
+__device__ __forceinline__ double2 w16<0>(double2 a) { return a; }
+template <>
+__device__ __forceinline__ double2 w16<1>(double2 a) {
+    return make_double2(a.x * kC16 + a.y * kS16, a.y * kC16 - a.x * kS16);
+}
+template <>
+__device__ __forceinline__ double2 w16<2>(double2 a) { return make_double2(kR2 * (a.x + a.y), kR2 * (a.y - a.x)); }
+template <>
+__device__ __forceinline__ double2 w16<3>(double2 a) {
+    return make_double2(a.x * kS16 + a.y * kC16, a.y * kS16 - a.x * kC16);
+}
+template <>
+__device__ __forceinline__ double2 w16<4>(double2 a) { return mul_mi(a); }
+template <>
+__device__ __forceinline__ double2 w16<6>(double2 a) { return make_double2(kR2 * (a.y - a.x), -kR2 * (a.x + a.y)); }
+template <>
+__device__ __forceinline__ double2 w16<9>(double2 a) {
+    return make_double2(-a.x * kC16 - a.y * kS16, a.x * kS16 - a.y * kC16);
+}
+
+__device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2, double2 &a3) {
+    const double2 t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = mul_mi(a1 - a3);
+    a0 = t0 + t2;
+    a2 = t0 - t2;
+    a1 = t1 + t3;
+    a3 = t1 - t3;
+}
+
+template <int R>
+struct DftC;
+
+template <>
+struct DftC<4> {
+    static __device__ __forceinline__ void run(double2 *v) { dft4(v[0], v[1], v[2], v[3]); }
+};
+
+template <>
+struct DftC<2> {
+    static __device__ __forceinline__ void run(double2 *v) {
+        const double2 a = v[0], b = v[1];
+        v[0] = a + b;
+        v[1] = a - b;
+    }
+};
+
+// 8 = 4 x 2: n = 2 n1 + n2, k = k1 + 4 k2
+template <>
+struct DftC<8> {
+    static __device__ __forceinline__ void run(double2 *v) {
+        double2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];  // n2 = 0
+        double2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];  // n2 = 1
+        dft4(a0, a1, a2, a3);
+        dft4(b0, b1, b2, b3);
+        b1 = w16<2>(b1);  // W8^1
+        b2 = mul_mi(b2);  // W8^2
+        b3 = w16<6>(b3);  // W8^3
+        v[0] = a0 + b0;
+        v[4] = a0 - b0;
+        v[1] = a1 + b1;
+        v[5] = a1 - b1;
+        v[2] = a2 + b2;
+        v[6] = a2 - b2;
+        v[3] = a3 + b3;
+        v[7] = a3 - b3;
+    }
+};
+
+// 16 = 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
+template <>
+struct DftC<16> {
+    static __device__ __forceinline__ void run(double2 *v) {
+        double2 a[4][4];  // a[n2][k1]
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+            a[n2][0] = v[n2];
+            a[n2][1] = v[4 + n2];
+            a[n2][2] = v[8 + n2];
+            a[n2][3] = v[12 + n2];
+            dft4(a[n2][0], a[n2][1], a[n2][2], a[n2][3]);
+        }
+        a[1][1] = w16<1>(a[1][1]);
+        a[1][2] = w16<2>(a[1][2]);
+        a[1][3] = w16<3>(a[1][3]);
+        a[2][1] = w16<2>(a[2][1]);
+        a[2][2] = w16<4>(a[2][2]);
+        a[2][3] = w16<6>(a[2][3]);
+        a[3][1] = w16<3>(a[3][1]);
+        a[3][2] = w16<6>(a[3][2]);
+        a[3][3] = w16<9>(a[3][3]);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            double2 b0 = a[0][k1], b1 = a[1][k1], b2 = a[2][k1], b3 = a[3][k1];
+            dft4(b0, b1, b2, b3);
+            v[k1] = b0;
+            v[k1 + 4] = b1;
+            v[k1 + 8] = b2;
+            v[k1 + 12] = b3;
+        }
+    }
+};
+
+// ---- compile-time plans ----
+// Every stage has NB = M/R butterflies with NB % 16 == 0 and a stride NS that
+// is 1 or a multiple of 16, so all padded shared-memory offsets of a stage are
+// compile-time constants added to one per-thread base.
+template <int M>
+struct Pow2Plan;
+template <>
+struct Pow2Plan<1024> {
+    static constexpr int TPF = 64;
+    static constexpr int R0 = 16, R1 = 16, R2 = 4;
+};
+template <>
+struct Pow2Plan<512> {
+    static constexpr int TPF = 64;
+    static constexpr int R0 = 16, R1 = 8, R2 = 4;
+};
+template <>
+struct Pow2Plan<256> {
+    static constexpr int TPF = 32;
+    static constexpr int R0 = 16, R1 = 4, R2 = 4;
+};
+
+// padded offset of (base + c) given that base % 16 == b16 is known to leave room
+template <int NS, int R, int r>
+struct WriteOff {
+    // NS == 1: targets R j + r with (R j) % 16 + r < 16 -> base + r
+    // NS % 16 == 0: targets d + r NS -> pad(d) + r NS 17/16
+    static constexpr int value = NS == 1 ? r : r * NS * 17 / 16;
+};
+
+// One Stockham stage with compile-time sizes on a padded buffer.
+template <int M, int R, int NS, int TPF>
+__device__ __forceinline__ void stage_ct(double2 *buf, const double2 *__restrict__ tw, int t) {
+    constexpr int NB = M / R;
+    constexpr int K = NB >= TPF ? NB / TPF : 1;  // butterflies per thread
+    constexpr bool ALL = NB >= TPF;              // every thread has a butterfly
+    constexpr int TWS = M / (NS * R);
+    static_assert((NB % TPF == 0 || TPF % NB == 0) && NB % 16 == 0, "stage layout");
+    static_assert(NS == 1 || NS % 16 == 0, "stage stride");
+    static_assert(NS != 1 || 16 % R == 0, "first-stage radix");
+    constexpr int RSTEP = NB * 17 / 16;  // padded distance between the R inputs
+    double2 v[K][R];
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (!ALL && j >= NB) break;
+        const int k = j % NS;
+        double2 w[R];
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) w[r] = __ldg(&tw[r * k * TWS]);
+        }
+        const double2 *src = buf + pad16(j);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[kb][r] = src[r * RSTEP];
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[kb][r] = cmul(v[kb][r], w[r]);
+        }
+        DftC<R>::run(v[kb]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (!ALL && j >= NB) break;
+        const int k = j % NS;
+        double2 *dst = buf + pad16((j / NS) * NS * R + k);
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[NS == 1 ? r : r * NS * 17 / 16] = v[kb][r];
+    }
+    __syncthreads();
+}
+
+template <int M>
+struct Pow2Dst {
+    using P = Pow2Plan<M>;
+    static constexpr int TPF = P::TPF;
+    static constexpr int NWARP = TPF / 32;
+    static __host__ __device__ constexpr int smem_len(int) { return padded_len(M); }
+
+    static __device__ __forceinline__ int idx(int i) { return pad16(i); }
+
+    static __device__ __forceinline__ void fft(double2 *buf, const double2 *__restrict__ tw, int t) {
+        stage_ct<M, P::R0, 1, TPF>(buf, tw, t);
+        stage_ct<M, P::R1, P::R0, TPF>(buf, tw, t);
+        stage_ct<M, P::R2, P::R0 * P::R1, TPF>(buf, tw, t);
+        static_assert(P::R0 * P::R1 * P::R2 == M, "plan must factor M");
+    }
+
+    // pre-twiddle in place; buf[1..M-1] hold z, buf[0], buf[M] are read as 0
+    static __device__ __forceinline__ void pre(double2 *buf, const double *__restrict__ sn, int t) {
+        constexpr int H = M / 2;
+#pragma unroll
+        for (int j = t; j <= H; j += TPF) {
+            if (j == 0) {
+                buf[0] = make_double2(0.0, 0.0);
+            } else if (j == H) {
+                const double2 z = buf[pad16(H)];
+                buf[pad16(H)] = __ldg(&sn[H]) * (z + z);
+            } else {
+                const double s = __ldg(&sn[j]);
+                const double2 a = buf[pad16(j)], b = buf[pad16(M - j)];
+                buf[pad16(j)] = s * (a + b) + 0.5 * (a - b);
+                buf[pad16(M - j)] = s * (a + b) + 0.5 * (b - a);
+            }
+        }
+        __syncthreads();
+    }
+
+    // post-processing: V in buf[0..M) -> y in buf[1..M-1]; buf[0] = buf[M] = 0.
+    // Thread t owns the E = H/TPF consecutive k in [t E, t E + E): a sequential
+    // scan of its segment, one warp shuffle scan of the segment totals, and one
+    // block barrier for the warp totals.
+    static __device__ __forceinline__ void post(double2 *buf, int t, double2 *wt) {
+        constexpr int H = M / 2;
+        constexpr int E = H / TPF;
+        static_assert(E >= 1 && H % TPF == 0, "scan layout");
+        const int lane = t & 31, w = t >> 5;
+        const int k0 = t * E;
+        double2 odd[E], even[E];
+        double2 run = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int k = k0 + e;
+            const double2 Vk = buf[pad16(k)];
+            const double2 Vm = buf[pad16(M - k)];  // k == 0 reads buf[M] = V_M, unused
+            if (k == 0) {
+                run = Vk;
+                even[e] = make_double2(0.0, 0.0);
+            } else {
+                run = run + (Vk + Vm);
+                const double2 d = Vk - Vm;
+                even[e] = make_double2(-d.y, d.x);
+            }
+            odd[e] = run;
+        }
+        double2 incl = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double ux = __shfl_up_sync(0xffffffffu, incl.x, o);
+            const double uy = __shfl_up_sync(0xffffffffu, incl.y, o);
+            if (lane >= o) incl = incl + make_double2(ux, uy);
+        }
+        double2 excl;
+        excl.x = __shfl_up_sync(0xffffffffu, incl.x, 1);
+        excl.y = __shfl_up_sync(0xffffffffu, incl.y, 1);
+        if (lane == 0) excl = make_double2(0.0, 0.0);
+        if (NWARP > 1 && lane == 31) wt[w] = incl;
+        __syncthreads();  // all reads of V done; warp totals visible
+#pragma unroll
+        for (int q = 0; q < NWARP - 1; ++q)
+            if (q < w) excl = excl + wt[q];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int k = k0 + e;
+            buf[pad16(2 * k + 1)] = odd[e] + excl;
+            if (k > 0) buf[pad16(2 * k)] = even[e];
+        }
+        if (t == 0) {
+            buf[0] = make_double2(0.0, 0.0);
+            buf[pad16(M)] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+    }
+
+    static __device__ __forceinline__ void dst(double2 *buf, const Plan &pl, int t, double2 *wt) {
+        pre(buf, pl.sn, t);
+        fft(buf, pl.tw, t);
+        post(buf, t, wt);
+    }
+};
+
+// The runtime mixed-radix transform behind the same interface (any even M <= 1024
+// of the form 2^a 3^b 5^c), unpadded.
+struct GenericDst {
+    static constexpr int TPF = kTPF;
+    static constexpr int NWARP = kTPF / 32;
+    static __host__ __device__ constexpr int smem_len(int m) { return m + 1; }
+    static __device__ __forceinline__ int idx(int i) { return i; }
+    static __device__ __forceinline__ void dst(double2 *buf, const Plan &pl, int t, double2 *wt) {
+        dst_inplace(buf, pl, t, wt);
+    }
+};
+
+}  // namespace ibpm

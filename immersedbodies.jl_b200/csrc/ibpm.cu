@@ -116,7 +116,8 @@ struct ibpm_handle {
     double fs_last[2] = {0, 0}, gm_last[6] = {0, 0, 0, 0, 0, 0};
     // work
     int kbatch = 1;  // columns per batch in the B setup
-    double *t1 = nullptr, *t2 = nullptr, *rhs = nullptr, *qs1 = nullptr, *Ftmp = nullptr, *part = nullptr;
+    double *t1 = nullptr, *t2 = nullptr, *rhs = nullptr, *rest = nullptr, *qs1 = nullptr, *Ftmp = nullptr;
+    double *part = nullptr;
     double *patch = nullptr;
     long long patch_stride = 0;
     double *Gw = nullptr, *psiw = nullptr, *qw = nullptr, *fcol = nullptr;  // batch work (K columns)
@@ -172,6 +173,10 @@ struct ibpm_handle {
     }
     ~ibpm_handle() {
         if (st) cudaStreamSynchronize(st);
+        for (int p = 0; p < 2; ++p) {
+            if (graph_exec[p]) cudaGraphExecDestroy(graph_exec[p]);
+            if (graph[p]) cudaGraphDestroy(graph[p]);
+        }
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         for (void *p : allocs) cudaFree(p);
         if (prm_h) cudaFreeHost(prm_h);
@@ -187,24 +192,84 @@ struct ibpm_handle {
     }
 
     // ---- line passes ----
-    template <class In, class Out>
-    void xpass(In in, Out out, int nbatch) {
+    // Dispatch on the transform length: compile-time power-of-two transforms
+    // for M in {128, 256, 512, 1024}, the runtime mixed-radix one otherwise.
+    template <class D, class In, class Out>
+    void xpass_t(In in, Out out, int nbatch) {
         const int pairs = (ny - 1 + 1) / 2;
         const dim3 grid((pairs + kNG - 1) / kNG, nbatch);
-        const size_t sm = (size_t)(kNG * (plx.M + 1) + 2 * kNG) * sizeof(double2);
+        const size_t sm = (size_t)(kNG * D::smem_len(plx.M) + D::NWARP * kNG) * sizeof(double2);
+        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, plx, ny - 1);
+    }
+    template <class In, class Out>
+    void xpass(In in, Out out, int nbatch) {
         const int pe = prof_begin();
-        xpass_kernel<kNG, In, Out><<<grid, kNG * kTPF, sm, st>>>(in, out, plx, ny - 1);
+        switch (plx.M) {
+            case 1024: xpass_t<Pow2Dst<1024>>(in, out, nbatch); break;
+            case 512: xpass_t<Pow2Dst<512>>(in, out, nbatch); break;
+            case 256: xpass_t<Pow2Dst<256>>(in, out, nbatch); break;
+            default: xpass_t<GenericDst>(in, out, nbatch); break;
+        }
         check_launch();
         prof_end(pe, IBPM_KCLASS_XPASS, 16.0 * (double)ng * nbatch);
     }
-    void ypass(const double *in, double *out, long long bs, int nbatch, Mult m) {
+    template <class D>
+    void ypass_t(const double *in, double *out, long long bs, int nbatch, Mult m) {
         const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nbatch);
-        const size_t sm = (size_t)(kNG * (ply.M + 1) + 2 * kNG) * sizeof(double2);
+        const size_t sm = (size_t)(kNG * D::smem_len(ply.M) + D::NWARP * kNG) * sizeof(double2);
+        ypass_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(in, out, bs, nx - 1, ply, m);
+    }
+    void ypass(const double *in, double *out, long long bs, int nbatch, Mult m) {
         const int pe = prof_begin();
-        ypass_kernel<kNG><<<grid, kNG * kTPF, sm, st>>>(in, out, bs, nx - 1, ply, m);
+        switch (ply.M) {
+            case 1024: ypass_t<Pow2Dst<1024>>(in, out, bs, nbatch, m); break;
+            case 512: ypass_t<Pow2Dst<512>>(in, out, bs, nbatch, m); break;
+            case 256: ypass_t<Pow2Dst<256>>(in, out, bs, nbatch, m); break;
+            default: ypass_t<GenericDst>(in, out, bs, nbatch, m); break;
+        }
         check_launch();
         prof_end(pe, IBPM_KCLASS_YPASS, 16.0 * (double)ng * nbatch);
     }
+    // Merged trial solve over all L levels: Gamma_new = Ainv(A Gamma + rest)
+    template <class D>
+    void trial_t(const double *Gold, const double *rest_, double *Gnew) {
+        {
+            const dim3 grid((ny - 1 + kNG - 1) / kNG, L);
+            const size_t sm = (size_t)(kNG * D::smem_len(plx.M) + D::NWARP * kNG) * sizeof(double2);
+            const int pe = prof_begin();
+            xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1, t2, ng, nx - 1, plx, ny - 1);
+            check_launch();
+            prof_end(pe, IBPM_KCLASS_XPASS, 32.0 * (double)ng * L);
+        }
+        {
+            const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), L);
+            const size_t sm = (size_t)(2 * kNG * D::smem_len(ply.M) + D::NWARP * kNG) * sizeof(double2);
+            // the cap must cover the largest M this instantiation serves (kMaxM)
+            static bool attr = false;
+            if (!attr) {
+                const int cap = (int)((2 * kNG * D::smem_len(kMaxM) + D::NWARP * kNG) * sizeof(double2));
+                CK(cudaFuncSetAttribute(ypass_trial_kernel<D, kNG>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+                attr = true;
+            }
+            const int pe = prof_begin();
+            ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1, t2, rhs, ng, nx - 1, ply,
+                                                                       mult(MULT_AIMPL, 1, 1));
+            check_launch();
+            prof_end(pe, IBPM_KCLASS_YPASS, 24.0 * (double)ng * L);
+        }
+        xpass(in_plain(rhs, ng), out_plain(Gnew, ng), L);
+    }
+    void trial(const double *Gold, const double *rest_, double *Gnew) {
+        if (plx.M == 1024 && ply.M == 1024)
+            trial_t<Pow2Dst<1024>>(Gold, rest_, Gnew);
+        else if (plx.M == 512 && ply.M == 512)
+            trial_t<Pow2Dst<512>>(Gold, rest_, Gnew);
+        else if (plx.M == 256 && ply.M == 256)
+            trial_t<Pow2Dst<256>>(Gold, rest_, Gnew);
+        else
+            trial_t<GenericDst>(Gold, rest_, Gnew);
+    }
+
     Mult mult(int mode, int lev0, int levstep) const {
         Mult m;
         m.mode = mode;
@@ -242,9 +307,10 @@ struct ibpm_handle {
             ypass(t1, t2, ng, nbatch, mult(MULT_LAPINV, 1, 0));
             xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch);
             if (curl_all || lev == 1) {
-                const dim3 grd((unsigned)((nq + 255) / 256), nbatch);
+                const dim3 blk(64, 4);
+                const dim3 grd((nx + 1 + 63) / 64, (ny + 3) / 4 + (ny + 1 + 3) / 4, nbatch);
                 const int pe = prof_begin();
-                curl_kernel<<<grd, 256, 0, st>>>(qout + (lev - 1) * nq, qbs, Pl, bs, lev < L ? psi_ + lev * ng : nullptr,
+                curl_kernel<<<grd, blk, 0, st>>>(qout + (lev - 1) * nq, qbs, Pl, bs, lev < L ? psi_ + lev * ng : nullptr,
                                                  bs, g);
                 check_launch();
                 prof_end(pe, IBPM_KCLASS_CURL, 8.0 * (double)(ng + nq) * nbatch);
@@ -315,11 +381,18 @@ struct ibpm_handle {
     void build_Binv();
     int cg(double *x, const double *b);
     void step(const ibpm_step_params &prm_in);
+    void step_body();
+    // CUDA graphs of step_body (static bodies), one per buffer parity
+    bool use_graphs = true;
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    long long graph_launches[2] = {0, 0};
     void materialise_q0();
 };
 
 void ibpm_handle::setup() {
     CK(cudaSetDevice(device));
+    if (const char *e = getenv("IBPM_NO_GRAPHS")) use_graphs = e[0] == '0';
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     if (!make_plan(nx, plx) || !make_plan(ny, ply))
         throw ApiError{IBPM_ERR_INVALID, "nx and ny must be even, <= 1024 and of the form 2^a 3^b 5^c"};
@@ -385,6 +458,7 @@ void ibpm_handle::setup() {
     t1 = dalloc<double>(ng * kb);
     t2 = dalloc<double>(ng * kb);
     rhs = dalloc<double>(ng * L);
+    rest = dalloc<double>(ng * L);
     qs1 = dalloc<double>(nq);
     Ftmp = dalloc<double>(2 * np);
     const int nchunk = (2 * np + 63) / 64;
@@ -556,24 +630,55 @@ void ibpm_handle::step(const ibpm_step_params &sp) {
     }
     q0_zero = false;
     q0_from_user = false;
+    // Static bodies: the rest of the step is one CUDA graph per parity of the
+    // ping-ponged Gamma / nonlin buffers (gc == nc always), captured on first use.
+    if (static_bodies && use_graphs && !prof) {
+        const int p = gc;
+        if (!graph_exec[p]) {
+            const int gc0 = gc, nc0 = nc;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            try {
+                step_body();
+            } catch (...) {
+                cudaGraph_t gdrop = nullptr;
+                cudaStreamEndCapture(st, &gdrop);
+                if (gdrop) cudaGraphDestroy(gdrop);
+                (void)cudaGetLastError();
+                gc = gc0;
+                nc = nc0;
+                throw;
+            }
+            CK(cudaStreamEndCapture(st, &graph[p]));
+            CK(cudaGraphInstantiate(&graph_exec[p], graph[p], 0));
+            gc = gc0;
+            nc = nc0;
+        }
+        CK(cudaGraphLaunch(graph_exec[p], st));
+        launches += graph_launches[p];
+        gc = 1 - gc;
+        nc = 1 - nc;
+        last_cg_iters = 0;
+        return;
+    }
+    step_body();
+}
+
+// The device work of one step after the per-step parameters are uploaded.
+void ibpm_handle::step_body() {
+    const long long launches0 = launches;
     double *Gold = G[gc], *Gnew = G[1 - gc];
     double *N1 = nl[nc], *N2 = nl[1 - nc];
     // get_trial_state (src/fluid.jl:467-506), all levels at once: the levels
     // only read the previous step's Gamma and q.
     {
-        NonlinArgs a{q, Gold, N1, prm, g};
+        NonlinArgs a{q, Gold, N1, N2, rest, prm, g};
         const dim3 blk(32, 8), grd((nx - 1 + 31) / 32, (ny - 1 + 7) / 8, L);
         const int pe = prof_begin();
         nonlinear_kernel<<<grd, blk, 0, st>>>(a);
         check_launch();
-        prof_end(pe, IBPM_KCLASS_NONLINEAR, 8.0 * (double)(nq + 2 * ng) * L);
+        prof_end(pe, IBPM_KCLASS_NONLINEAR, 8.0 * (double)(nq + 4 * ng) * L);
     }
-    xpass(in_plain(Gold, ng), out_plain(t1, ng), L);
-    ypass(t1, t2, ng, L, mult(MULT_AEXPL, 1, 1));
-    xpass(in_plain(t2, ng), OutTrialRhs{rhs, N1, N2, Gold, ng, g}, L);
-    xpass(in_plain(rhs, ng), out_plain(t1, ng), L);
-    ypass(t1, t2, ng, L, mult(MULT_AIMPL, 1, 1));
-    xpass(in_plain(t2, ng), out_plain(Gnew, ng), L);
+    trial(Gold, rest, Gnew);
     nc = 1 - nc;  // _cycle!(state.nonlin)
     vort2flux(psi, qs1, Gnew, 0, 0, 1, false);
     // couple_surface_rigid (src/coupling.jl:236-250)
@@ -602,6 +707,7 @@ void ibpm_handle::step(const ibpm_step_params &sp) {
     // vort2flux!(state.psi, state.q, state.Gamma)
     vort2flux(psi, q, Gnew, 0, 0, 1, true);
     gc = 1 - gc;
+    graph_launches[1 - gc] = launches - launches0;
 }
 
 namespace {

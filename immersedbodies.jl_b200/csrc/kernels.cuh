@@ -2,7 +2,7 @@
 // stencils, B^-1 algebra).  Included by ibpm.cu only.
 #pragma once
 #include "common.cuh"
-#include "fft_dst.cuh"
+#include "fft_pow2.cuh"
 
 namespace ibpm {
 
@@ -87,6 +87,18 @@ struct OutTrialRhs {
     }
 };
 
+// 1/d: the hardware reciprocal approximation refined by two Newton-Raphson
+// steps (e = 1 - d y, y += y e); within an ulp or two of the correctly rounded
+// quotient, for the positive, normal d of the spectral multipliers.
+__device__ __forceinline__ double recip(double d) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    double e = fma(-d, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-d, y, 1.0);
+    return fma(y, e, y);
+}
+
 // Spectral multipliers scale / Lambda (src/fluid.jl:117-134)
 enum { MULT_LAPINV = 0, MULT_AEXPL = 1, MULT_AIMPL = 2 };
 struct Mult {
@@ -96,45 +108,48 @@ struct Mult {
     double scale;       // 1 / (4 nx ny)
     double h, Re, dt;
     int lev0, levstep;  // level of batch b: lev0 + b * levstep
-    __device__ __forceinline__ double operator()(int b, int i, int j) const {
-        const double lam = -2 * ((__ldg(&cx[i]) + __ldg(&cy[j])) - 2);
-        if (mode == MULT_LAPINV) return scale / lam;
+    // c = dt / (2 Re hc^2) of the batch's level; the reference's (lam dt) / (2 Re hc^2)
+    // becomes lam c (within one rounding), which leaves one division per element.
+    __device__ __forceinline__ double coef(int b) const {
         const int lev = lev0 + b * levstep;
         const double hc = ldexp(h, lev - 1);
-        const double den = 2 * Re * (hc * hc);
-        if (mode == MULT_AEXPL) {
-            const double Lam = 1.0 / (1 - lam * dt / den);
-            return scale / Lam;
-        }
-        const double Lam = 1 + lam * dt / den;
-        return scale / Lam;
+        return dt / (2 * Re * (hc * hc));
+    }
+    __device__ __forceinline__ double operator()(double c, int i, int j) const {
+        const double lam = -2 * ((__ldg(&cx[i]) + __ldg(&cy[j])) - 2);
+        if (mode == MULT_LAPINV) return scale * recip(lam);
+        if (mode == MULT_AEXPL) return scale * (1 - lam * c);  // scale / (1 / (1 - lam c))
+        return scale * recip(1 + lam * c);
     }
 };
 
 // X pass: DST along x of rows (ja, jb) = (2p+1, 2p+2) of each batch field.
-template <int NG, class In, class Out>
-__global__ void __launch_bounds__(kTPF *NG) xpass_kernel(In in, Out out, Plan pl, int nrows) {
+// D is the line transform (Pow2Dst<M> or GenericDst); NG line pairs per block.
+template <class D, int NG, class In, class Out>
+__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) xpass_kernel(In in, Out out, Plan pl, int nrows) {
     extern __shared__ double2 smem[];
+    constexpr int TPF = D::TPF;
     const int M = pl.M;
-    const int g = threadIdx.x / kTPF, t = threadIdx.x % kTPF;
-    double2 *buf = smem + g * (M + 1);
-    double2 *wt = smem + NG * (M + 1) + 2 * g;
+    const int G = D::smem_len(M);
+    const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
+    double2 *buf = smem + g * G;
+    double2 *wt = smem + NG * G + D::NWARP * g;
     const int b = blockIdx.y;
     const int pair = blockIdx.x * NG + g;
     const int ja = 2 * pair + 1, jb = 2 * pair + 2;
     const bool va = ja <= nrows, vb = jb <= nrows;
-    for (int i = t; i <= M; i += kTPF) {
+    for (int i = t; i <= M; i += TPF) {
         double2 z = make_double2(0.0, 0.0);
         if (i >= 1 && i < M) {
             if (va) z.x = in(b, i, ja);
             if (vb) z.y = in(b, i, jb);
         }
-        buf[i] = z;
+        buf[D::idx(i)] = z;
     }
     __syncthreads();
-    dst_inplace(buf, pl, t, wt);
-    for (int i = 1 + t; i < M; i += kTPF) {
-        const double2 y = buf[i];
+    D::dst(buf, pl, t, wt);
+    for (int i = 1 + t; i < M; i += TPF) {
+        const double2 y = buf[D::idx(i)];
         if (va) out(b, i, ja, y.x);
         if (vb) out(b, i, jb, y.y);
     }
@@ -142,14 +157,16 @@ __global__ void __launch_bounds__(kTPF *NG) xpass_kernel(In in, Out out, Plan pl
 
 // Y pass: for each column i, x[i, :] = DST_y(mult(i, :) * DST_y(in[i, :])).
 // A block owns 2*NG adjacent columns; loads and stores are row-coalesced.
-template <int NG>
-__global__ void __launch_bounds__(kTPF *NG) ypass_kernel(const double *__restrict__ in, double *__restrict__ out,
-                                                         long long bs, int ncols, Plan pl, Mult mult) {
+template <class D, int NG>
+__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) ypass_kernel(const double *__restrict__ in, double *__restrict__ out,
+                                                           long long bs, int ncols, Plan pl, Mult mult) {
     extern __shared__ double2 smem[];
+    constexpr int TPF = D::TPF;
     const int M = pl.M;
-    const int g = threadIdx.x / kTPF, t = threadIdx.x % kTPF;
-    double2 *buf = smem + g * (M + 1);
-    double2 *wt = smem + NG * (M + 1) + 2 * g;
+    const int G = D::smem_len(M);
+    const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
+    double2 *buf = smem + g * G;
+    double2 *wt = smem + NG * G + D::NWARP * g;
     const int b = blockIdx.y;
     const int c0 = blockIdx.x * 2 * NG;  // 0-based first column of the block
     const double *src = in + b * bs;
@@ -160,28 +177,140 @@ __global__ void __launch_bounds__(kTPF *NG) ypass_kernel(const double *__restric
         const int col = c0 + c;
         double v = 0.0;
         if (jj >= 1 && jj < M && col < ncols) v = src[col + (long long)ncols * (jj - 1)];
-        double *slot = reinterpret_cast<double *>(smem + (c >> 1) * (M + 1) + jj) + (c & 1);
+        double *slot = reinterpret_cast<double *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
         *slot = v;
     }
     __syncthreads();
-    dst_inplace(buf, pl, t, wt);
-    {
+    // DST, spectral multiply, DST; one loop body so the transform is emitted once
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        D::dst(buf, pl, t, wt);
+        if (pass == 1) break;
         const int ia = c0 + 2 * g + 1, ib = c0 + 2 * g + 2;  // 1-based columns
-        for (int jj = 1 + t; jj < M; jj += kTPF) {
-            double2 y = buf[jj];
-            y.x *= (ia <= ncols) ? mult(b, ia, jj) : 0.0;
-            y.y *= (ib <= ncols) ? mult(b, ib, jj) : 0.0;
-            buf[jj] = y;
+        const double cb = mult.coef(b);
+        for (int jj = 1 + t; jj < M; jj += TPF) {
+            double2 y = buf[D::idx(jj)];
+            y.x *= (ia <= ncols) ? mult(cb, ia, jj) : 0.0;
+            y.y *= (ib <= ncols) ? mult(cb, ib, jj) : 0.0;
+            buf[D::idx(jj)] = y;
         }
+        __syncthreads();
     }
-    __syncthreads();
-    dst_inplace(buf, pl, t, wt);
     for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
         const int c = e % W, jj = e / W;
         const int col = c0 + c;
         if (jj >= 1 && jj < M && col < ncols) {
-            const double *slot = reinterpret_cast<const double *>(smem + (c >> 1) * (M + 1) + jj) + (c & 1);
+            const double *slot = reinterpret_cast<const double *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
             dst[col + (long long)ncols * (jj - 1)] = *slot;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Merged trial solve of get_trial_state (src/fluid.jl:485-496):
+//   Gamma_s = Ainv (A Gamma + rest),  rest = dt (1.5 N1 - 0.5 N2) + rhsbc.
+// With S the 2D DST-I and S S = 1/scale:  S(A Gamma) = S(Gamma) / Lambda_e, so
+//   Gamma_s = S( scale / Lambda_i * ( S(Gamma) / Lambda_e + S(rest) ) ),
+// three passes instead of the reference's four transforms in six passes.
+// ---------------------------------------------------------------------------
+
+// X pass: row j of level b as one complex line z = Gamma + i rest.
+template <class D, int NG>
+__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
+    xpass_trial_kernel(const double *__restrict__ gam, const double *__restrict__ rest, double *__restrict__ t1,
+                       double *__restrict__ t2, long long bs, int ld, Plan pl, int nrows) {
+    extern __shared__ double2 smem[];
+    constexpr int TPF = D::TPF;
+    const int M = pl.M;
+    const int G = D::smem_len(M);
+    const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
+    double2 *buf = smem + g * G;
+    double2 *wt = smem + NG * G + D::NWARP * g;
+    const int b = blockIdx.y;
+    const int j = blockIdx.x * NG + g + 1;
+    const bool valid = j <= nrows;
+    const long long row = b * bs + (long long)ld * (j - 1);
+    for (int i = t; i <= M; i += TPF) {
+        double2 z = make_double2(0.0, 0.0);
+        if (valid && i >= 1 && i < M) z = make_double2(gam[row + i - 1], rest[row + i - 1]);
+        buf[D::idx(i)] = z;
+    }
+    __syncthreads();
+    D::dst(buf, pl, t, wt);
+    if (valid)
+        for (int i = 1 + t; i < M; i += TPF) {
+            const double2 y = buf[D::idx(i)];
+            t1[row + i - 1] = y.x;
+            t2[row + i - 1] = y.y;
+        }
+}
+
+// Y pass: a block owns 2NG adjacent columns.  Phase 1 transforms each column's
+// (S_x Gamma, S_x rest) pair as one complex line and combines
+//   v = scale / Lambda_i * (S Gamma / Lambda_e + S rest)
+//     = (S Gamma (1 - lam c) + S rest) * scale / (1 + lam c),   c = dt / (2 Re hc^2);
+// phase 2 transforms the real v of two columns packed as one complex line.
+template <class D, int NG>
+__global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
+    ypass_trial_kernel(const double *__restrict__ t1, const double *__restrict__ t2, double *__restrict__ out,
+                       long long bs, int ncols, Plan pl, Mult mult) {
+    extern __shared__ double2 smem[];
+    constexpr int TPF = D::TPF;
+    constexpr int W = 2 * NG;
+    const int M = pl.M;
+    const int G = D::smem_len(M);
+    const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
+    double2 *wt = smem + W * G + D::NWARP * g;
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * W;  // 0-based first column
+    const double *s1 = t1 + b * bs, *s2 = t2 + b * bs;
+    double *dst = out + b * bs;
+    for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
+        const int c = e % W, jj = e / W;
+        const int col = c0 + c;
+        double2 z = make_double2(0.0, 0.0);
+        if (jj >= 1 && jj < M && col < ncols) {
+            const long long o = col + (long long)ncols * (jj - 1);
+            z = make_double2(s1[o], s2[o]);
+        }
+        smem[c * G + D::idx(jj)] = z;
+    }
+    __syncthreads();
+    const double cb = mult.coef(b);
+    const double scale = mult.scale;
+#pragma unroll 1
+    for (int r = 0; r < 2; ++r) {
+        const int c = r * NG + g;
+        double2 *buf = smem + c * G;
+        D::dst(buf, pl, t, wt);
+        const int col1 = c0 + c + 1;  // 1-based column
+        const bool ok = col1 <= ncols;
+        const double cxv = ok ? __ldg(&mult.cx[col1]) : 0.0;
+        for (int jj = 1 + t; jj < M; jj += TPF) {
+            const double2 y = buf[D::idx(jj)];
+            double v = 0.0;
+            if (ok) {
+                const double lam = -2 * ((cxv + __ldg(&mult.cy[jj])) - 2);
+                v = (y.x * (1 - lam * cb) + y.y) * (scale * recip(1 + lam * cb));
+            }
+            buf[D::idx(jj)] = make_double2(v, 0.0);
+        }
+        __syncthreads();
+    }
+    // phase 2: pack columns (2g, 2g+1) into buffer 2g
+    {
+        double2 *ba = smem + (2 * g) * G;
+        const double2 *bb = smem + (2 * g + 1) * G;
+        for (int jj = 1 + t; jj < M; jj += TPF) ba[D::idx(jj)].y = bb[D::idx(jj)].x;
+        __syncthreads();
+        D::dst(ba, pl, t, wt);
+    }
+    for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
+        const int c = e % W, jj = e / W;
+        const int col = c0 + c;
+        if (jj >= 1 && jj < M && col < ncols) {
+            const double2 y = smem[(c & ~1) * G + D::idx(jj)];
+            dst[col + (long long)ncols * (jj - 1)] = (c & 1) ? y.y : y.x;
         }
     }
 }
@@ -196,6 +325,8 @@ struct NonlinArgs {
     const double *q;      // nq x L
     const double *gam;    // ng x L
     double *out;          // ng x L (state.nonlin[1])
+    const double *n2;     // ng x L (state.nonlin[2]); with rest != nullptr
+    double *rest;         // ng x L: dt (1.5 N1 - 0.5 N2) + rhsbc, or nullptr
     const StepDev *prm;
     Grid g;
 };
@@ -243,23 +374,38 @@ __global__ void nonlinear_kernel(NonlinArgs a) {
     // rot! at Gamma(I, J) with i = I+1, j = J+1 (fluid.jl:106-108)
     const double r = (fqx(I + 1, J) - fqx(I + 1, J + 1)) + (fqy(I + 1, J + 1) - fqy(I, J + 1));
     const double hc = gridstep(g, lev);
-    a.out[b * ng + GI(I, J)] = r * (1 / (hc * hc));
+    const double n1 = r * (1 / (hc * hc));
+    a.out[b * ng + GI(I, J)] = n1;
+    if (a.rest) {
+        // rest = dt b1 N1 + dt b2 N2 + rhsbc (fluid.jl:487-493), rhsbc = apply_bc!(0, get_bc(..); fac)
+        double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * a.n2[b * ng + GI(I, J)];
+        if (lev < g.L && on_ring(g, I, J)) {
+            const double fac = 0.25 * g.dt / (g.Re * (hc * hc));
+            v = v + apply_bc_at(0.0, C, g, I, J, fac);
+        }
+        a.rest[b * ng + GI(I, J)] = v;
+    }
 }
 
 // 4-argument curl! (src/fluid.jl:230-276) with psi_bc = get_bc(psi_coarse) (zero if null).
-// One thread per face; batch b uses psi + b*bs, q + b*qbs, coarse + b*cbs.
+// A 2D grid over the faces: blockIdx.y < ceil((ny+1)/by) covers the x faces
+// (rows j <= ny) and, offset by that count, the y faces (rows j <= ny+1).
+// Batch b (blockIdx.z) uses psi + b*bs, q + b*qbs, coarse + b*cbs.
 __global__ void curl_kernel(double *__restrict__ qout, long long qbs, const double *__restrict__ psi, long long bs,
                             const double *__restrict__ coarse, long long cbs, Grid g) {
     const int nx = g.nx, ny = g.ny;
-    const long long nu = (long long)(nx + 1) * ny, nq = nu + (long long)nx * (ny + 1);
-    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = blockIdx.y;
-    if (f >= nq) return;
+    const long long nu = (long long)(nx + 1) * ny;
+    const int rows_u = (ny + blockDim.y - 1) / blockDim.y;
+    const bool yface = (int)blockIdx.y >= rows_u;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = (yface ? blockIdx.y - rows_u : blockIdx.y) * blockDim.y + threadIdx.y + 1;
+    const int b = blockIdx.z;
     const double *P = psi + b * bs;
     const double *C = coarse ? coarse + b * cbs : nullptr;
-    double v;
-    if (f < nu) {
-        const int i = (int)(f % (nx + 1)) + 1, j = (int)(f / (nx + 1)) + 1;
+    double *q = qout + b * qbs;
+    if (!yface) {
+        if (i > nx + 1 || j > ny) return;
+        double v;
         if (i == 1)
             v = getbc(C, g, SIDE_L, j + 1) - getbc(C, g, SIDE_L, j);
         else if (i == nx + 1)
@@ -270,9 +416,10 @@ __global__ void curl_kernel(double *__restrict__ qout, long long qbs, const doub
             v = getbc(C, g, SIDE_T, i) - P[GI(i - 1, ny - 1)];
         else
             v = P[GI(i - 1, j)] - P[GI(i - 1, j - 1)];
+        q[UI(i, j)] = v;
     } else {
-        const long long k = f - nu;
-        const int i = (int)(k % nx) + 1, j = (int)(k / nx) + 1;
+        if (i > nx || j > ny + 1) return;
+        double v;
         if (j == 1)
             v = getbc(C, g, SIDE_B, i) - getbc(C, g, SIDE_B, i + 1);
         else if (j == ny + 1)
@@ -283,8 +430,8 @@ __global__ void curl_kernel(double *__restrict__ qout, long long qbs, const doub
             v = P[GI(nx - 1, j - 1)] - getbc(C, g, SIDE_R, j);
         else
             v = P[GI(i - 1, j - 1)] - P[GI(i, j - 1)];
+        q[VI(i, j)] = v;
     }
-    qout[b * qbs + f] = v;
 }
 
 // coarsify! (src/fluid.jl:208-228): fine level -> central block of the next coarser level.
