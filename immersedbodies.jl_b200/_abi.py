@@ -21,6 +21,7 @@ IBPM_ERR_REGION = -3
 IBPM_ERR_NOMEM = -4
 IBPM_ERR_NONFINITE = -5
 IBPM_FP64 = 0
+IBPM_FP32 = 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

@@ -7,11 +7,29 @@
 //   y flux  nx x (ny+1):                VI(i,j) = nu + (i-1) + nx(j-1)
 // A "batch" index b selects a field: either the level (b = lev-1, the trial
 // solves) or an independent right-hand side (the B^-1 setup columns).
+//
+// Fields have element type T: double for the plain FP64 path, float for the
+// mixed-precision path.  Boundary values, base fluxes and coupling sums are
+// always accumulated in double.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace ibpm {
+
+// complex type of a real type
+template <class T>
+struct Cx;
+template <>
+struct Cx<double> {
+    using type = double2;
+    static __host__ __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct Cx<float> {
+    using type = float2;
+    static __host__ __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); }
+};
 
 struct Grid {
     int nx, ny, L;
@@ -35,24 +53,26 @@ __device__ __forceinline__ double gridstep(const Grid &g, int lev) { return ldex
 
 // get_bc! (src/fluid.jl:278-306), one entry: rbc[side offset + ibc] from the
 // coarser level's field r.  r == nullptr means zero boundary values.
-__device__ __forceinline__ double getbc(const double *__restrict__ r, const Grid &g, int side, int ibc) {
+template <class T>
+__device__ __forceinline__ double getbc(const T *__restrict__ r, const Grid &g, int side, int ibc) {
     if (r == nullptr) return 0.0;
     const int nx = g.nx, ny = g.ny;
     if (side == SIDE_B || side == SIDE_T) {
         const int row = side == SIDE_B ? ny / 4 : 3 * ny / 4;
-        if (ibc & 1) return r[GI(nx / 4 + (ibc - 1) / 2, row)];
+        if (ibc & 1) return (double)r[GI(nx / 4 + (ibc - 1) / 2, row)];
         const int i = nx / 4 + ibc / 2;
-        return 0.5 * (r[GI(i, row)] + r[GI(i - 1, row)]);
+        return 0.5 * ((double)r[GI(i, row)] + (double)r[GI(i - 1, row)]);
     }
     const int col = side == SIDE_L ? nx / 4 : 3 * nx / 4;
-    if (ibc & 1) return r[GI(col, ny / 4 + (ibc - 1) / 2)];
+    if (ibc & 1) return (double)r[GI(col, ny / 4 + (ibc - 1) / 2)];
     const int j = ny / 4 + ibc / 2;
-    return 0.5 * (r[GI(col, j)] + r[GI(col, j - 1)]);
+    return 0.5 * ((double)r[GI(col, j)] + (double)r[GI(col, j - 1)]);
 }
 
 // apply_bc! contribution at (i, j) (src/fluid.jl:308-338), accumulated in the
 // reference's order (bottom/top rows first, then left/right columns).
-__device__ __forceinline__ double apply_bc_at(double v, const double *__restrict__ r, const Grid &g, int i, int j,
+template <class T>
+__device__ __forceinline__ double apply_bc_at(double v, const T *__restrict__ r, const Grid &g, int i, int j,
                                               double fac) {
     if (j == 1) v += fac * getbc(r, g, SIDE_B, i + 1);
     if (j == g.ny - 1) v += fac * getbc(r, g, SIDE_T, i + 1);
@@ -106,15 +126,16 @@ struct Panels {
 
 // Regularised flux on the panels' bounding box (compact patch):
 // patch[(i - i0) + pw (j - j0)] for x faces, offset pw*ph for y faces.
+template <class T>
 struct Patch {
-    const double *p;
+    const T *p;
     const int *bbox;      // device: i0, i1, j0, j1 (1-based face indices)
     long long bs;
     __device__ __forceinline__ double get(int b, int comp, int i, int j) const {
         const int i0 = bbox[0], i1 = bbox[1], j0 = bbox[2], j1 = bbox[3];
         if (i < i0 || i > i1 || j < j0 || j > j1) return 0.0;
         const int pw = i1 - i0 + 1, ph = j1 - j0 + 1;
-        return p[b * bs + (long long)comp * pw * ph + (i - i0) + (long long)pw * (j - j0)];
+        return (double)p[b * bs + (long long)comp * pw * ph + (i - i0) + (long long)pw * (j - j0)];
     }
 };
 

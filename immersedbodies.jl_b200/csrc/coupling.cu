@@ -119,8 +119,9 @@ __global__ void bbox_kernel(Panels P, Grid g) {
 // tile, then every face sums w * f over that list in panel order -- the same
 // accumulation order as the reference's sequential loop over panels.
 // f: 2np per batch (x block then y block); patch output per batch.
+template <class T>
 __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *__restrict__ f, long long fbs,
-                                                        double *__restrict__ patch, long long pbs) {
+                                                        T *__restrict__ patch, long long pbs) {
     __shared__ int list[1024];
     __shared__ int warp_cnt[8];
     __shared__ int total;
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *
     const int ti1 = min(ti0 + kTile - 1, i1), tj1 = min(tj0 + kTile - 1, j1);
     const int b = blockIdx.z;
     const double *fb = f + b * fbs;
-    double *out = patch + b * pbs;
+    T *out = patch + b * pbs;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int li = tid % kTile, lj = tid / kTile;
     const int i = ti0 + li, j = tj0 + lj;
@@ -173,15 +174,16 @@ __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *
         __syncthreads();
     }
     if (i <= ti1 && j <= tj1) {
-        out[(i - i0) + (long long)pw * (j - j0)] = accx;
-        out[(long long)pw * ph + (i - i0) + (long long)pw * (j - j0)] = accy;
+        out[(i - i0) + (long long)pw * (j - j0)] = (T)accx;
+        out[(long long)pw * ph + (i - i0) + (long long)pw * (j - j0)] = (T)accy;
     }
 }
 
 // regT! (src/coupling.jl:57-69): fb[p, c] = dot(q_c[7x7 at p], w[p, c]) in
 // column-major order.  With add_q0 it is couple_surface_rigid's
 // Ftmp = E (qs + q0) - ub h (src/coupling.jl:239-244).
-__global__ void regT_kernel(Panels P, const double *__restrict__ q, long long qbs, double *__restrict__ out,
+template <class T>
+__global__ void regT_kernel(Panels P, const T *__restrict__ q, long long qbs, double *__restrict__ out,
                             long long obs, int nbatch, int add_q0, const StepDev *__restrict__ prm, Grid g) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int np = P.np;
@@ -189,14 +191,14 @@ __global__ void regT_kernel(Panels P, const double *__restrict__ q, long long qb
     const int b = t / (2 * np), pcomp = t % (2 * np);
     const int c = pcomp / np, p = pcomp % np;
     const long long nu = (long long)(g.nx + 1) * g.ny;
-    const double *Q = q + b * qbs;
+    const T *Q = q + b * qbs;
     const int i0 = P.pc[2 * p] - 3, j0 = P.pc[2 * p + 1] - 3;
     const double *w = P.w + (long long)(p * 2 + c) * 49;
     double s = 0.0;
     for (int bb = 0; bb < 7; ++bb)
         for (int a = 0; a < 7; ++a) {
             const int i = i0 + a, j = j0 + bb;
-            double v = c == 0 ? Q[UI(i, j)] : Q[VI(i, j)];
+            double v = c == 0 ? (double)Q[UI(i, j)] : (double)Q[VI(i, j)];
             if (add_q0) v = v + (c == 0 ? base_flux_x(g, prm, 1, i, j) : base_flux_y(g, prm, 1, i, j));
             s += v * w[bb * 7 + a];
         }
@@ -226,16 +228,26 @@ void launch_reg_weights(const Panels &P, int p0, int p1, const Grid &g, cudaStre
     if (p1 > p0) reg_weights_kernel<<<p1 - p0, dim3(49, 2), 0, st>>>(P, p0, g);
 }
 void launch_bbox(const Panels &P, const Grid &g, cudaStream_t st) { bbox_kernel<<<1, 256, 0, st>>>(P, g); }
-void launch_reg_patch(const Panels &P, const double *f, long long fbs, double *patch, long long pbs, int nbatch,
+template <class T>
+void launch_reg_patch(const Panels &P, const double *f, long long fbs, T *patch, long long pbs, int nbatch,
                       const Grid &g, cudaStream_t st) {
     const int tiles_x = (g.nx + 1 + kTile - 1) / kTile + 1, tiles_y = (g.ny + 1 + kTile - 1) / kTile + 1;
-    reg_patch_kernel<<<dim3(tiles_x, tiles_y, nbatch), 256, 0, st>>>(P, f, fbs, patch, pbs);
+    reg_patch_kernel<T><<<dim3(tiles_x, tiles_y, nbatch), 256, 0, st>>>(P, f, fbs, patch, pbs);
 }
-void launch_regT(const Panels &P, const double *q, long long qbs, double *out, long long obs, int nbatch, int add_q0,
+template <class T>
+void launch_regT(const Panels &P, const T *q, long long qbs, double *out, long long obs, int nbatch, int add_q0,
                  const StepDev *prm, const Grid &g, cudaStream_t st) {
     const int nt = 2 * P.np * nbatch;
-    regT_kernel<<<(nt + 127) / 128, 128, 0, st>>>(P, q, qbs, out, obs, nbatch, add_q0, prm, g);
+    regT_kernel<T><<<(nt + 127) / 128, 128, 0, st>>>(P, q, qbs, out, obs, nbatch, add_q0, prm, g);
 }
+template void launch_reg_patch<double>(const Panels &, const double *, long long, double *, long long, int,
+                                       const Grid &, cudaStream_t);
+template void launch_reg_patch<float>(const Panels &, const double *, long long, float *, long long, int,
+                                      const Grid &, cudaStream_t);
+template void launch_regT<double>(const Panels &, const double *, long long, double *, long long, int, int,
+                                  const StepDev *, const Grid &, cudaStream_t);
+template void launch_regT<float>(const Panels &, const float *, long long, double *, long long, int, int,
+                                 const StepDev *, const Grid &, cudaStream_t);
 void launch_rigid_motion(const Panels &P, const double *ref_xb, const double *motion, int p0, int p1,
                          cudaStream_t st) {
     if (p1 > p0) rigid_motion_kernel<<<(p1 - p0 + 127) / 128, 128, 0, st>>>(P, ref_xb, motion, p0, p1);

@@ -8,9 +8,13 @@ constexpr int kTile = 16;  // faces per side of a reg! gather tile
 
 void launch_reg_weights(const Panels &P, int p0, int p1, const Grid &g, cudaStream_t st);
 void launch_bbox(const Panels &P, const Grid &g, cudaStream_t st);
-void launch_reg_patch(const Panels &P, const double *f, long long fbs, double *patch, long long pbs, int nbatch,
+// reg! onto a patch of element type T (double or float); forces f are double.
+template <class T>
+void launch_reg_patch(const Panels &P, const double *f, long long fbs, T *patch, long long pbs, int nbatch,
                       const Grid &g, cudaStream_t st);
-void launch_regT(const Panels &P, const double *q, long long qbs, double *out, long long obs, int nbatch, int add_q0,
+// regT! from a level-1 flux of element type T, summed in double.
+template <class T>
+void launch_regT(const Panels &P, const T *q, long long qbs, double *out, long long obs, int nbatch, int add_q0,
                  const StepDev *prm, const Grid &g, cudaStream_t st);
 void launch_rigid_motion(const Panels &P, const double *ref_xb, const double *motion, int p0, int p1,
                          cudaStream_t st);

@@ -10,13 +10,19 @@
 // z = a + i b, pre-twiddled with v_j = sin(pi j/M)(z_j + z_{M-j}) + (z_j - z_{M-j})/2.
 // With V = FFT(v):  y_1 = V_0,  y_{2k} = i (V_k - V_{M-k}),
 //                   y_{2k+1} = y_{2k-1} + V_k + V_{M-k}  (a prefix scan),
-// and DST(a) = Re y, DST(b) = Im y.  The FFT is a mixed-radix (4, 2, 3, 5)
-// Stockham transform held in shared memory; each stage keeps its butterflies
-// in registers between one read phase and one write phase, so a line needs a
-// single (M+1)-entry buffer.
+// and DST(a) = Re y, DST(b) = Im y.  This file holds the runtime mixed-radix
+// (4, 2, 3, 5) Stockham transform for any even M = 2^a 3^b 5^c <= 1024; each
+// stage keeps its butterflies in registers between one read phase and one write
+// phase, so a line needs a single (M+1)-entry buffer.  fft_pow2.cuh holds the
+// compile-time power-of-two transforms behind the same interface.
+//
+// Element type T is double or float; the prefix scan always accumulates in
+// double (its partial sums are larger than its outputs).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include "common.cuh"
 
 namespace ibpm {
 
@@ -26,40 +32,57 @@ constexpr int kMaxE = 8;        // scan values per thread (M/2/kTPF, M <= 1024)
 constexpr int kMaxStages = 12;
 constexpr int kMaxM = 1024;     // largest transform length (nx or ny)
 
-struct Plan {
+template <class T>
+struct PlanT {
+    using C = typename Cx<T>::type;
     int M;                      // transform length (nx or ny); DST length M-1
     int nst;                    // number of FFT stages
     int radix[kMaxStages];
-    const double2 *tw;          // tw[k] = exp(-2 pi i k / M), k < M
-    const double *sn;           // sn[j] = sin(pi j / M), j <= M
+    const C *tw;                // tw[k] = exp(-2 pi i k / M), k < M
+    const T *sn;                // sn[j] = sin(pi j / M), j <= M
 };
 
-__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
 // multiply by -i
 __device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }
+__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d2(float2 a) { return make_double2(a.x, a.y); }
+template <class C>
+__device__ __forceinline__ C from_d2(double2 a);
+template <>
+__device__ __forceinline__ double2 from_d2<double2>(double2 a) { return a; }
+template <>
+__device__ __forceinline__ float2 from_d2<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
 
-template <int R>
+template <int R, class C>
 struct Dft;
 
-template <>
-struct Dft<2> {
-    static __device__ __forceinline__ void run(double2 *v) {
-        const double2 a = v[0], b = v[1];
+template <class C>
+struct Dft<2, C> {
+    static __device__ __forceinline__ void run(C *v) {
+        const C a = v[0], b = v[1];
         v[0] = a + b;
         v[1] = a - b;
     }
 };
 
-template <>
-struct Dft<4> {
-    static __device__ __forceinline__ void run(double2 *v) {
-        const double2 t0 = v[0] + v[2], t1 = v[0] - v[2];
-        const double2 t2 = v[1] + v[3], t3 = mul_mi(v[1] - v[3]);
+template <class C>
+struct Dft<4, C> {
+    static __device__ __forceinline__ void run(C *v) {
+        const C t0 = v[0] + v[2], t1 = v[0] - v[2];
+        const C t2 = v[1] + v[3], t3 = mul_mi(v[1] - v[3]);
         v[0] = t0 + t2;
         v[2] = t0 - t2;
         v[1] = t1 + t3;
@@ -67,32 +90,34 @@ struct Dft<4> {
     }
 };
 
-template <>
-struct Dft<3> {
-    static __device__ __forceinline__ void run(double2 *v) {
-        const double s3 = 0.86602540378443864676;  // sin(2 pi / 3)
-        const double2 a1 = v[1] + v[2], d1 = v[1] - v[2];
-        const double2 x0 = v[0] + a1;
-        const double2 t = v[0] - 0.5 * a1;
-        const double2 u = mul_mi(s3 * d1);
+template <class C>
+struct Dft<3, C> {
+    static __device__ __forceinline__ void run(C *v) {
+        using R = decltype(C().x);
+        const R s3 = (R)0.86602540378443864676;  // sin(2 pi / 3)
+        const C a1 = v[1] + v[2], d1 = v[1] - v[2];
+        const C x0 = v[0] + a1;
+        const C t = v[0] - (R)0.5 * a1;
+        const C u = mul_mi(s3 * d1);
         v[0] = x0;
         v[1] = t + u;
         v[2] = t - u;
     }
 };
 
-template <>
-struct Dft<5> {
-    static __device__ __forceinline__ void run(double2 *v) {
-        const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;  // cos(2pi/5), cos(4pi/5)
-        const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;   // sin(2pi/5), sin(4pi/5)
-        const double2 b1 = v[1] + v[4], b2 = v[2] + v[3];
-        const double2 d1 = v[1] - v[4], d2 = v[2] - v[3];
-        const double2 x0 = v[0] + b1 + b2;
-        const double2 e1 = v[0] + c1 * b1 + c2 * b2;
-        const double2 e2 = v[0] + c2 * b1 + c1 * b2;
-        const double2 f1 = mul_mi(s1 * d1 + s2 * d2);
-        const double2 f2 = mul_mi(s2 * d1 - s1 * d2);
+template <class C>
+struct Dft<5, C> {
+    static __device__ __forceinline__ void run(C *v) {
+        using R = decltype(C().x);
+        const R c1 = (R)0.30901699437494742410, c2 = (R)-0.80901699437494742410;  // cos(2pi/5), cos(4pi/5)
+        const R s1 = (R)0.95105651629515357212, s2 = (R)0.58778525229247312917;   // sin(2pi/5), sin(4pi/5)
+        const C b1 = v[1] + v[4], b2 = v[2] + v[3];
+        const C d1 = v[1] - v[4], d2 = v[2] - v[3];
+        const C x0 = v[0] + b1 + b2;
+        const C e1 = v[0] + c1 * b1 + c2 * b2;
+        const C e2 = v[0] + c2 * b1 + c1 * b2;
+        const C f1 = mul_mi(s1 * d1 + s2 * d2);
+        const C f2 = mul_mi(s2 * d1 - s1 * d2);
         v[0] = x0;
         v[1] = e1 + f1;
         v[4] = e1 - f1;
@@ -103,12 +128,12 @@ struct Dft<5> {
 
 // One Stockham stage of radix R over buf[0..M).  Every thread of the block
 // must call it (it contains block barriers).
-template <int R>
-__device__ __forceinline__ void fft_stage(double2 *buf, int M, int Ns, const double2 *__restrict__ tw, int t) {
+template <int R, class C>
+__device__ __forceinline__ void fft_stage(C *buf, int M, int Ns, const C *__restrict__ tw, int t) {
     constexpr int KMAX = kMaxV / R;
     const int nb = M / R;
     const int twstep = M / (Ns * R);
-    double2 v[KMAX][R];
+    C v[KMAX][R];
     int dst[KMAX];
 #pragma unroll
     for (int kb = 0; kb < KMAX; ++kb) {
@@ -119,7 +144,7 @@ __device__ __forceinline__ void fft_stage(double2 *buf, int M, int Ns, const dou
             v[kb][0] = buf[j];
 #pragma unroll
             for (int r = 1; r < R; ++r) v[kb][r] = cmul(buf[j + r * nb], __ldg(&tw[r * k * twstep]));
-            Dft<R>::run(v[kb]);
+            Dft<R, C>::run(v[kb]);
             dst[kb] = (j / Ns) * Ns * R + k;
         }
     }
@@ -135,37 +160,41 @@ __device__ __forceinline__ void fft_stage(double2 *buf, int M, int Ns, const dou
 }
 
 // Forward complex FFT of buf[0..M) in place (natural order in and out).
-__device__ __forceinline__ void fft(double2 *buf, const Plan &pl, int t) {
+template <class T>
+__device__ __forceinline__ void fft(typename Cx<T>::type *buf, const PlanT<T> &pl, int t) {
+    using C = typename Cx<T>::type;
     int Ns = 1;
     for (int s = 0; s < pl.nst; ++s) {
         const int R = pl.radix[s];
         if (R == 4)
-            fft_stage<4>(buf, pl.M, Ns, pl.tw, t);
+            fft_stage<4, C>(buf, pl.M, Ns, pl.tw, t);
         else if (R == 2)
-            fft_stage<2>(buf, pl.M, Ns, pl.tw, t);
+            fft_stage<2, C>(buf, pl.M, Ns, pl.tw, t);
         else if (R == 3)
-            fft_stage<3>(buf, pl.M, Ns, pl.tw, t);
+            fft_stage<3, C>(buf, pl.M, Ns, pl.tw, t);
         else
-            fft_stage<5>(buf, pl.M, Ns, pl.tw, t);
+            fft_stage<5, C>(buf, pl.M, Ns, pl.tw, t);
         Ns *= R;
     }
 }
 
 // DST pre-twiddle in place: buf[1..M-1] holds z, buf[0] and buf[M] are read as 0.
-__device__ __forceinline__ void dst_pre(double2 *buf, const Plan &pl, int t) {
+template <class T>
+__device__ __forceinline__ void dst_pre(typename Cx<T>::type *buf, const PlanT<T> &pl, int t) {
+    using C = typename Cx<T>::type;
     const int M = pl.M, H = M >> 1;
     for (int j = t; j <= H; j += kTPF) {
         if (j == 0) {
-            buf[0] = make_double2(0.0, 0.0);
+            buf[0] = Cx<T>::make(0, 0);
         } else if (j == H) {
-            const double2 z = buf[H];
-            const double s = __ldg(&pl.sn[H]);
+            const C z = buf[H];
+            const T s = __ldg(&pl.sn[H]);
             buf[H] = s * (z + z);
         } else {
-            const double2 a = buf[j], b = buf[M - j];
-            const double s = __ldg(&pl.sn[j]);
-            buf[j] = s * (a + b) + 0.5 * (a - b);
-            buf[M - j] = s * (a + b) + 0.5 * (b - a);
+            const C a = buf[j], b = buf[M - j];
+            const T s = __ldg(&pl.sn[j]);
+            buf[j] = s * (a + b) + (T)0.5 * (a - b);
+            buf[M - j] = s * (a + b) + (T)0.5 * (b - a);
         }
     }
     __syncthreads();
@@ -173,26 +202,29 @@ __device__ __forceinline__ void dst_pre(double2 *buf, const Plan &pl, int t) {
 
 // DST post-processing: buf[0..M) holds V; on return buf[1..M-1] holds y and
 // buf[0] = buf[M] = 0.  wt: two double2 scratch slots for this group.
-__device__ __forceinline__ void dst_post(double2 *buf, const Plan &pl, int t, double2 *wt) {
+template <class T>
+__device__ __forceinline__ void dst_post(typename Cx<T>::type *buf, const PlanT<T> &pl, int t, double2 *wt) {
+    using C = typename Cx<T>::type;
     const int M = pl.M, H = M >> 1;
     const int E = (H + kTPF - 1) / kTPF;
     const int k0 = t * E;
-    double2 c[kMaxE], ev[kMaxE];
+    double2 c[kMaxE];
+    C ev[kMaxE];
     double2 run = make_double2(0.0, 0.0);
 #pragma unroll
     for (int e = 0; e < kMaxE; ++e) {
         const int k = k0 + e;
         c[e] = make_double2(0.0, 0.0);
-        ev[e] = make_double2(0.0, 0.0);
+        ev[e] = Cx<T>::make(0, 0);
         if (e < E && k < H) {
-            const double2 Vk = buf[k];
+            const C Vk = buf[k];
             if (k == 0) {
-                run = Vk;
+                run = to_d2(Vk);
             } else {
-                const double2 Vm = buf[M - k];
-                run = run + (Vk + Vm);
-                const double2 d = Vk - Vm;
-                ev[e] = make_double2(-d.y, d.x);  // i (V_k - V_{M-k})
+                const C Vm = buf[M - k];
+                run = run + to_d2(Vk + Vm);
+                const C d = Vk - Vm;
+                ev[e] = Cx<T>::make(-d.y, d.x);  // i (V_k - V_{M-k})
             }
             c[e] = run;
         }
@@ -217,22 +249,23 @@ __device__ __forceinline__ void dst_post(double2 *buf, const Plan &pl, int t, do
     for (int e = 0; e < kMaxE; ++e) {
         const int k = k0 + e;
         if (e < E && k < H) {
-            buf[2 * k + 1] = (t == 0 && e == 0) ? c[e] : c[e] + excl;
+            buf[2 * k + 1] = from_d2<C>(c[e] + excl);
             if (k > 0) buf[2 * k] = ev[e];
         }
     }
     if (t == 0) {
-        buf[0] = make_double2(0.0, 0.0);
-        buf[M] = make_double2(0.0, 0.0);
+        buf[0] = Cx<T>::make(0, 0);
+        buf[M] = Cx<T>::make(0, 0);
     }
     __syncthreads();
 }
 
 // Full DST-I of the packed lines in buf[1..M-1] (in place).
-__device__ __forceinline__ void dst_inplace(double2 *buf, const Plan &pl, int t, double2 *wt) {
-    dst_pre(buf, pl, t);
-    fft(buf, pl, t);
-    dst_post(buf, pl, t, wt);
+template <class T>
+__device__ __forceinline__ void dst_inplace(typename Cx<T>::type *buf, const PlanT<T> &pl, int t, double2 *wt) {
+    dst_pre<T>(buf, pl, t);
+    fft<T>(buf, pl, t);
+    dst_post<T>(buf, pl, t, wt);
 }
 
 }  // namespace ibpm

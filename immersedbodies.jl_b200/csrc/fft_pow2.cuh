@@ -7,6 +7,7 @@
 // strides and index splits are constants, the shared buffer is padded by one
 // complex per 16 to keep the strided Stockham writes free of bank conflicts,
 // and the post-processing scan runs on warp shuffles with one block barrier.
+// T (double or float) is the element type; the scan accumulates in double.
 #pragma once
 #include "fft_dst.cuh"
 
@@ -23,60 +24,88 @@ constexpr double kC16 = 0.92387953251128675613;  // cos(pi/8)
 constexpr double kS16 = 0.38268343236508977173;  // sin(pi/8)
 
 // multiply by W16^m for the exponents the radix-16 butterfly needs
-template <int m>
-__device__ __forceinline__ double2 w16(double2 a);
-template <>
-__device__ __forceinline__ double2 w16<0>(double2 a) { return a; }
-template <>
-__device__ __forceinline__ double2 w16<1>(double2 a) {
-    return make_double2(a.x * kC16 + a.y * kS16, a.y * kC16 - a.x * kS16);
-}
-template <>
-__device__ __forceinline__ double2 w16<2>(double2 a) { return make_double2(kR2 * (a.x + a.y), kR2 * (a.y - a.x)); }
-template <>
-__device__ __forceinline__ double2 w16<3>(double2 a) {
-    return make_double2(a.x * kS16 + a.y * kC16, a.y * kS16 - a.x * kC16);
-}
-template <>
-__device__ __forceinline__ double2 w16<4>(double2 a) { return mul_mi(a); }
-template <>
-__device__ __forceinline__ double2 w16<6>(double2 a) { return make_double2(kR2 * (a.y - a.x), -kR2 * (a.x + a.y)); }
-template <>
-__device__ __forceinline__ double2 w16<9>(double2 a) {
-    return make_double2(-a.x * kC16 - a.y * kS16, a.x * kS16 - a.y * kC16);
+template <int m, class C>
+struct W16;
+template <class C>
+struct W16<0, C> {
+    static __device__ __forceinline__ C mul(C a) { return a; }
+};
+template <class C>
+struct W16<1, C> {
+    static __device__ __forceinline__ C mul(C a) {
+        using R = decltype(C().x);
+        return C{a.x * (R)kC16 + a.y * (R)kS16, a.y * (R)kC16 - a.x * (R)kS16};
+    }
+};
+template <class C>
+struct W16<2, C> {
+    static __device__ __forceinline__ C mul(C a) {
+        using R = decltype(C().x);
+        return C{(R)kR2 * (a.x + a.y), (R)kR2 * (a.y - a.x)};
+    }
+};
+template <class C>
+struct W16<3, C> {
+    static __device__ __forceinline__ C mul(C a) {
+        using R = decltype(C().x);
+        return C{a.x * (R)kS16 + a.y * (R)kC16, a.y * (R)kS16 - a.x * (R)kC16};
+    }
+};
+template <class C>
+struct W16<4, C> {
+    static __device__ __forceinline__ C mul(C a) { return mul_mi(a); }
+};
+template <class C>
+struct W16<6, C> {
+    static __device__ __forceinline__ C mul(C a) {
+        using R = decltype(C().x);
+        return C{(R)kR2 * (a.y - a.x), -(R)kR2 * (a.x + a.y)};
+    }
+};
+template <class C>
+struct W16<9, C> {
+    static __device__ __forceinline__ C mul(C a) {
+        using R = decltype(C().x);
+        return C{-a.x * (R)kC16 - a.y * (R)kS16, a.x * (R)kS16 - a.y * (R)kC16};
+    }
+};
+template <int m, class C>
+__device__ __forceinline__ C w16(C a) {
+    return W16<m, C>::mul(a);
 }
 
-__device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2, double2 &a3) {
-    const double2 t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = mul_mi(a1 - a3);
+template <class C>
+__device__ __forceinline__ void dft4(C &a0, C &a1, C &a2, C &a3) {
+    const C t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = mul_mi(a1 - a3);
     a0 = t0 + t2;
     a2 = t0 - t2;
     a1 = t1 + t3;
     a3 = t1 - t3;
 }
 
-template <int R>
+template <int R, class C>
 struct DftC;
 
-template <>
-struct DftC<4> {
-    static __device__ __forceinline__ void run(double2 *v) { dft4(v[0], v[1], v[2], v[3]); }
+template <class C>
+struct DftC<4, C> {
+    static __device__ __forceinline__ void run(C *v) { dft4(v[0], v[1], v[2], v[3]); }
 };
 
-template <>
-struct DftC<2> {
-    static __device__ __forceinline__ void run(double2 *v) {
-        const double2 a = v[0], b = v[1];
+template <class C>
+struct DftC<2, C> {
+    static __device__ __forceinline__ void run(C *v) {
+        const C a = v[0], b = v[1];
         v[0] = a + b;
         v[1] = a - b;
     }
 };
 
 // 8 = 4 x 2: n = 2 n1 + n2, k = k1 + 4 k2
-template <>
-struct DftC<8> {
-    static __device__ __forceinline__ void run(double2 *v) {
-        double2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];  // n2 = 0
-        double2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];  // n2 = 1
+template <class C>
+struct DftC<8, C> {
+    static __device__ __forceinline__ void run(C *v) {
+        C a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];  // n2 = 0
+        C b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];  // n2 = 1
         dft4(a0, a1, a2, a3);
         dft4(b0, b1, b2, b3);
         b1 = w16<2>(b1);  // W8^1
@@ -94,10 +123,10 @@ struct DftC<8> {
 };
 
 // 16 = 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
-template <>
-struct DftC<16> {
-    static __device__ __forceinline__ void run(double2 *v) {
-        double2 a[4][4];  // a[n2][k1]
+template <class C>
+struct DftC<16, C> {
+    static __device__ __forceinline__ void run(C *v) {
+        C a[4][4];  // a[n2][k1]
 #pragma unroll
         for (int n2 = 0; n2 < 4; ++n2) {
             a[n2][0] = v[n2];
@@ -117,7 +146,7 @@ struct DftC<16> {
         a[3][3] = w16<9>(a[3][3]);
 #pragma unroll
         for (int k1 = 0; k1 < 4; ++k1) {
-            double2 b0 = a[0][k1], b1 = a[1][k1], b2 = a[2][k1], b3 = a[3][k1];
+            C b0 = a[0][k1], b1 = a[1][k1], b2 = a[2][k1], b3 = a[3][k1];
             dft4(b0, b1, b2, b3);
             v[k1] = b0;
             v[k1 + 4] = b1;
@@ -158,8 +187,8 @@ struct WriteOff {
 };
 
 // One Stockham stage with compile-time sizes on a padded buffer.
-template <int M, int R, int NS, int TPF>
-__device__ __forceinline__ void stage_ct(double2 *buf, const double2 *__restrict__ tw, int t) {
+template <int M, int R, int NS, int TPF, class C>
+__device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t) {
     constexpr int NB = M / R;
     constexpr int K = NB >= TPF ? NB / TPF : 1;  // butterflies per thread
     constexpr bool ALL = NB >= TPF;              // every thread has a butterfly
@@ -168,25 +197,25 @@ __device__ __forceinline__ void stage_ct(double2 *buf, const double2 *__restrict
     static_assert(NS == 1 || NS % 16 == 0, "stage stride");
     static_assert(NS != 1 || 16 % R == 0, "first-stage radix");
     constexpr int RSTEP = NB * 17 / 16;  // padded distance between the R inputs
-    double2 v[K][R];
+    C v[K][R];
 #pragma unroll
     for (int kb = 0; kb < K; ++kb) {
         const int j = t + kb * TPF;
         if (!ALL && j >= NB) break;
         const int k = j % NS;
-        double2 w[R];
+        C w[R];
         if (NS > 1) {
 #pragma unroll
             for (int r = 1; r < R; ++r) w[r] = __ldg(&tw[r * k * TWS]);
         }
-        const double2 *src = buf + pad16(j);
+        const C *src = buf + pad16(j);
 #pragma unroll
         for (int r = 0; r < R; ++r) v[kb][r] = src[r * RSTEP];
         if (NS > 1) {
 #pragma unroll
             for (int r = 1; r < R; ++r) v[kb][r] = cmul(v[kb][r], w[r]);
         }
-        DftC<R>::run(v[kb]);
+        DftC<R, C>::run(v[kb]);
     }
     __syncthreads();
 #pragma unroll
@@ -194,44 +223,46 @@ __device__ __forceinline__ void stage_ct(double2 *buf, const double2 *__restrict
         const int j = t + kb * TPF;
         if (!ALL && j >= NB) break;
         const int k = j % NS;
-        double2 *dst = buf + pad16((j / NS) * NS * R + k);
+        C *dst = buf + pad16((j / NS) * NS * R + k);
 #pragma unroll
         for (int r = 0; r < R; ++r) dst[NS == 1 ? r : r * NS * 17 / 16] = v[kb][r];
     }
     __syncthreads();
 }
 
-template <int M>
+template <int M, class T>
 struct Pow2Dst {
     using P = Pow2Plan<M>;
+    using Real = T;
+    using C = typename Cx<T>::type;
     static constexpr int TPF = P::TPF;
     static constexpr int NWARP = TPF / 32;
     static __host__ __device__ constexpr int smem_len(int) { return padded_len(M); }
 
     static __device__ __forceinline__ int idx(int i) { return pad16(i); }
 
-    static __device__ __forceinline__ void fft(double2 *buf, const double2 *__restrict__ tw, int t) {
-        stage_ct<M, P::R0, 1, TPF>(buf, tw, t);
-        stage_ct<M, P::R1, P::R0, TPF>(buf, tw, t);
-        stage_ct<M, P::R2, P::R0 * P::R1, TPF>(buf, tw, t);
+    static __device__ __forceinline__ void fft(C *buf, const C *__restrict__ tw, int t) {
+        stage_ct<M, P::R0, 1, TPF, C>(buf, tw, t);
+        stage_ct<M, P::R1, P::R0, TPF, C>(buf, tw, t);
+        stage_ct<M, P::R2, P::R0 * P::R1, TPF, C>(buf, tw, t);
         static_assert(P::R0 * P::R1 * P::R2 == M, "plan must factor M");
     }
 
     // pre-twiddle in place; buf[1..M-1] hold z, buf[0], buf[M] are read as 0
-    static __device__ __forceinline__ void pre(double2 *buf, const double *__restrict__ sn, int t) {
+    static __device__ __forceinline__ void pre(C *buf, const T *__restrict__ sn, int t) {
         constexpr int H = M / 2;
 #pragma unroll
         for (int j = t; j <= H; j += TPF) {
             if (j == 0) {
-                buf[0] = make_double2(0.0, 0.0);
+                buf[0] = Cx<T>::make(0, 0);
             } else if (j == H) {
-                const double2 z = buf[pad16(H)];
+                const C z = buf[pad16(H)];
                 buf[pad16(H)] = __ldg(&sn[H]) * (z + z);
             } else {
-                const double s = __ldg(&sn[j]);
-                const double2 a = buf[pad16(j)], b = buf[pad16(M - j)];
-                buf[pad16(j)] = s * (a + b) + 0.5 * (a - b);
-                buf[pad16(M - j)] = s * (a + b) + 0.5 * (b - a);
+                const T s = __ldg(&sn[j]);
+                const C a = buf[pad16(j)], b = buf[pad16(M - j)];
+                buf[pad16(j)] = s * (a + b) + (T)0.5 * (a - b);
+                buf[pad16(M - j)] = s * (a + b) + (T)0.5 * (b - a);
             }
         }
         __syncthreads();
@@ -241,26 +272,27 @@ struct Pow2Dst {
     // Thread t owns the E = H/TPF consecutive k in [t E, t E + E): a sequential
     // scan of its segment, one warp shuffle scan of the segment totals, and one
     // block barrier for the warp totals.
-    static __device__ __forceinline__ void post(double2 *buf, int t, double2 *wt) {
+    static __device__ __forceinline__ void post(C *buf, int t, double2 *wt) {
         constexpr int H = M / 2;
         constexpr int E = H / TPF;
         static_assert(E >= 1 && H % TPF == 0, "scan layout");
         const int lane = t & 31, w = t >> 5;
         const int k0 = t * E;
-        double2 odd[E], even[E];
+        double2 odd[E];
+        C even[E];
         double2 run = make_double2(0.0, 0.0);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = k0 + e;
-            const double2 Vk = buf[pad16(k)];
-            const double2 Vm = buf[pad16(M - k)];  // k == 0 reads buf[M] = V_M, unused
+            const C Vk = buf[pad16(k)];
+            const C Vm = buf[pad16(M - k)];  // k == 0 reads buf[M] = V_M, unused
             if (k == 0) {
-                run = Vk;
-                even[e] = make_double2(0.0, 0.0);
+                run = to_d2(Vk);
+                even[e] = Cx<T>::make(0, 0);
             } else {
-                run = run + (Vk + Vm);
-                const double2 d = Vk - Vm;
-                even[e] = make_double2(-d.y, d.x);
+                run = run + to_d2(Vk + Vm);
+                const C d = Vk - Vm;
+                even[e] = Cx<T>::make(-d.y, d.x);
             }
             odd[e] = run;
         }
@@ -283,17 +315,17 @@ struct Pow2Dst {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = k0 + e;
-            buf[pad16(2 * k + 1)] = odd[e] + excl;
+            buf[pad16(2 * k + 1)] = from_d2<C>(odd[e] + excl);
             if (k > 0) buf[pad16(2 * k)] = even[e];
         }
         if (t == 0) {
-            buf[0] = make_double2(0.0, 0.0);
-            buf[pad16(M)] = make_double2(0.0, 0.0);
+            buf[0] = Cx<T>::make(0, 0);
+            buf[pad16(M)] = Cx<T>::make(0, 0);
         }
         __syncthreads();
     }
 
-    static __device__ __forceinline__ void dst(double2 *buf, const Plan &pl, int t, double2 *wt) {
+    static __device__ __forceinline__ void dst(C *buf, const PlanT<T> &pl, int t, double2 *wt) {
         pre(buf, pl.sn, t);
         fft(buf, pl.tw, t);
         post(buf, t, wt);
@@ -302,13 +334,16 @@ struct Pow2Dst {
 
 // The runtime mixed-radix transform behind the same interface (any even M <= 1024
 // of the form 2^a 3^b 5^c), unpadded.
+template <class T>
 struct GenericDst {
+    using Real = T;
+    using C = typename Cx<T>::type;
     static constexpr int TPF = kTPF;
     static constexpr int NWARP = kTPF / 32;
     static __host__ __device__ constexpr int smem_len(int m) { return m + 1; }
     static __device__ __forceinline__ int idx(int i) { return i; }
-    static __device__ __forceinline__ void dst(double2 *buf, const Plan &pl, int t, double2 *wt) {
-        dst_inplace(buf, pl, t, wt);
+    static __device__ __forceinline__ void dst(C *buf, const PlanT<T> &pl, int t, double2 *wt) {
+        dst_inplace<T>(buf, pl, t, wt);
     }
 };
 

@@ -1,5 +1,7 @@
-// ibpm.cu -- libibpm_b200: the FP64 CNAB/IBPM time step on one B200, behind
-// the C ABI of include/ibpm_b200.h.
+// ibpm.cu -- libibpm_b200: the CNAB/IBPM time step on one B200, behind the C
+// ABI of include/ibpm_b200.h.  Engine<double> is the plain FP64 drop-in path;
+// Engine<float> is the mixed-precision path (FP32 fields and transforms, FP64
+// scans, boundary values, CG and force sums, and an FP64 B^-1).
 //
 // Device state per handle (column-major, the reference's State layout):
 //   q (nq x L), psi (ng x L), Gamma[2] (ng x L, ping-pong: state.Γ and the
@@ -16,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/ibpm_b200.h"
@@ -46,7 +49,20 @@ struct ApiError {
     std::string msg;
 };
 
-bool make_plan(int M, Plan &pl) {
+// Julia's shortest round-trip printing of a Float64 (for the reference's error text).
+std::string jl_float(double v) {
+    char buf[64];
+    for (int prec = 1; prec <= 17; ++prec) {
+        snprintf(buf, sizeof buf, "%.*g", prec, v);
+        if (strtod(buf, nullptr) == v) break;
+    }
+    std::string s(buf);
+    if (s.find_first_of(".eni") == std::string::npos) s += ".0";
+    return s;
+}
+
+template <class T>
+bool make_plan(int M, PlanT<T> &pl) {
     if (M < 4 || M > kMaxM || (M & 1)) return false;
     pl.M = M;
     pl.nst = 0;
@@ -84,7 +100,30 @@ bool make_plan(int M, Plan &pl) {
 
 }  // namespace
 
+// The C ABI's opaque handle: one engine of either precision.
 struct ibpm_handle {
+    std::string last_error;
+    virtual ~ibpm_handle() {}
+    virtual void set_state(const ibpm_state_view *s) = 0;
+    virtual void get_state(ibpm_state_view *s) = 0;
+    virtual bool advance(int64_t nsteps, const ibpm_step_params *params) = 0;  // true: CG hit maxiter
+    virtual void get_forces(double *fb, double *total) = 0;
+    virtual void get_time(int64_t *index, double *t) = 0;
+    virtual void get_info(ibpm_info *info) = 0;
+    virtual void *stream_ptr() = 0;
+    virtual long long launch_count() const = 0;
+    virtual void set_profile(int enable) = 0;
+    virtual void read_profile(int kclass, int64_t *launches, double *ms, double *bytes) = 0;
+    virtual void diag_solve(int op, int level, const double *b, double *x) = 0;
+    virtual void diag_apply_B(const double *z, double *x) = 0;
+    virtual void diag_binv(double *out) = 0;
+    virtual void diag_vort2flux(double *gamma, double *psi, double *q) = 0;
+    virtual void diag_reg(const double *f, double *gamma1, const double *q1, double *fout) = 0;
+};
+
+template <class T>
+struct Engine final : ibpm_handle {
+    using C = typename Cx<T>::type;
     // problem
     Grid g{};
     int nx = 0, ny = 0, L = 0, np = 0, nbody = 0;
@@ -96,16 +135,19 @@ struct ibpm_handle {
     int device = 0;
     cudaStream_t st = nullptr;
     // transforms
-    Plan plx{}, ply{};
-    double2 *twx = nullptr, *twy = nullptr;
-    double *snx = nullptr, *sny = nullptr, *cx = nullptr, *cy = nullptr;
+    PlanT<T> plx{}, ply{};
+    C *twx = nullptr, *twy = nullptr;
+    T *snx = nullptr, *sny = nullptr;
+    double *cx = nullptr, *cy = nullptr;
     // state
     int64_t index = 0;
     double t0 = 0.0;
-    double *q = nullptr, *psi = nullptr, *G[2] = {nullptr, nullptr}, *nl[2] = {nullptr, nullptr};
+    T *q = nullptr, *psi = nullptr, *G[2] = {nullptr, nullptr}, *nl[2] = {nullptr, nullptr};
     int gc = 0;  // state.Γ = G[gc]
     int nc = 0;  // state.nonlin[1] = nl[nc], state.nonlin[2] = nl[1 - nc]
-    double *q0mat = nullptr;
+    T *q0mat = nullptr;
+    double *stage = nullptr;  // double staging buffer for FP32 state transfers
+    size_t stage_len = 0;
     bool q0_from_user = false;
     bool q0_zero = true;  // State(prob) starts with q0 = 0 until the first step
     Panels P{};
@@ -116,11 +158,12 @@ struct ibpm_handle {
     double fs_last[2] = {0, 0}, gm_last[6] = {0, 0, 0, 0, 0, 0};
     // work
     int kbatch = 1;  // columns per batch in the B setup
-    double *t1 = nullptr, *t2 = nullptr, *rhs = nullptr, *rest = nullptr, *qs1 = nullptr, *Ftmp = nullptr;
-    double *part = nullptr;
-    double *patch = nullptr;
+    T *t1 = nullptr, *t2 = nullptr, *rhs = nullptr, *rest = nullptr, *qs1 = nullptr;
+    double *Ftmp = nullptr, *part = nullptr;
+    T *patch = nullptr;
     long long patch_stride = 0;
-    double *Gw = nullptr, *psiw = nullptr, *qw = nullptr, *fcol = nullptr;  // batch work (K columns)
+    T *Gw = nullptr, *psiw = nullptr, *qw = nullptr;  // batch work (K columns)
+    double *fcol = nullptr;
     double *Binv = nullptr, *rowk = nullptr, *colk = nullptr;
     double *cg_u = nullptr, *cg_r = nullptr, *cg_c = nullptr, *cg_s = nullptr, *cg_s_h = nullptr;
     int *err = nullptr, *err_h = nullptr;
@@ -158,20 +201,19 @@ struct ibpm_handle {
         prof_recs.push_back(ProfRec{cls, i, bytes});
     }
     std::vector<void *> allocs;
-    std::string last_error;
 
-    template <class T>
-    T *dalloc(size_t n) {
+    template <class U>
+    U *dalloc(size_t n) {
         void *p = nullptr;
         if (n == 0) n = 1;
-        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
-        if (e != cudaSuccess) throw ApiError{IBPM_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed"};
+        cudaError_t e = cudaMalloc(&p, n * sizeof(U));
+        if (e != cudaSuccess) throw ApiError{IBPM_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(U)) + " bytes failed"};
         allocs.push_back(p);
-        dev_bytes += (long long)(n * sizeof(T));
-        CK(cudaMemsetAsync(p, 0, n * sizeof(T), st));
-        return static_cast<T *>(p);
+        dev_bytes += (long long)(n * sizeof(U));
+        CK(cudaMemsetAsync(p, 0, n * sizeof(U), st));
+        return static_cast<U *>(p);
     }
-    ~ibpm_handle() {
+    ~Engine() override {
         if (st) cudaStreamSynchronize(st);
         for (int p = 0; p < 2; ++p) {
             if (graph_exec[p]) cudaGraphExecDestroy(graph_exec[p]);
@@ -183,6 +225,7 @@ struct ibpm_handle {
         if (motion_h) cudaFreeHost(motion_h);
         if (cg_s_h) cudaFreeHost(cg_s_h);
         if (err_h) cudaFreeHost(err_h);
+        if (st_side) cudaStreamDestroy(st_side);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -198,44 +241,44 @@ struct ibpm_handle {
     void xpass_t(In in, Out out, int nbatch) {
         const int pairs = (ny - 1 + 1) / 2;
         const dim3 grid((pairs + kNG - 1) / kNG, nbatch);
-        const size_t sm = (size_t)(kNG * D::smem_len(plx.M) + D::NWARP * kNG) * sizeof(double2);
+        const size_t sm = pass_smem<D>(plx.M, kNG, kNG);
         xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, plx, ny - 1);
     }
     template <class In, class Out>
     void xpass(In in, Out out, int nbatch) {
         const int pe = prof_begin();
         switch (plx.M) {
-            case 1024: xpass_t<Pow2Dst<1024>>(in, out, nbatch); break;
-            case 512: xpass_t<Pow2Dst<512>>(in, out, nbatch); break;
-            case 256: xpass_t<Pow2Dst<256>>(in, out, nbatch); break;
-            default: xpass_t<GenericDst>(in, out, nbatch); break;
+            case 1024: xpass_t<Pow2Dst<1024, T>>(in, out, nbatch); break;
+            case 512: xpass_t<Pow2Dst<512, T>>(in, out, nbatch); break;
+            case 256: xpass_t<Pow2Dst<256, T>>(in, out, nbatch); break;
+            default: xpass_t<GenericDst<T>>(in, out, nbatch); break;
         }
         check_launch();
         prof_end(pe, IBPM_KCLASS_XPASS, 16.0 * (double)ng * nbatch);
     }
     template <class D>
-    void ypass_t(const double *in, double *out, long long bs, int nbatch, Mult m) {
+    void ypass_t(const T *in, T *out, long long bs, int nbatch, Mult m) {
         const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nbatch);
-        const size_t sm = (size_t)(kNG * D::smem_len(ply.M) + D::NWARP * kNG) * sizeof(double2);
+        const size_t sm = pass_smem<D>(ply.M, kNG, kNG);
         ypass_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(in, out, bs, nx - 1, ply, m);
     }
-    void ypass(const double *in, double *out, long long bs, int nbatch, Mult m) {
+    void ypass(const T *in, T *out, long long bs, int nbatch, Mult m) {
         const int pe = prof_begin();
         switch (ply.M) {
-            case 1024: ypass_t<Pow2Dst<1024>>(in, out, bs, nbatch, m); break;
-            case 512: ypass_t<Pow2Dst<512>>(in, out, bs, nbatch, m); break;
-            case 256: ypass_t<Pow2Dst<256>>(in, out, bs, nbatch, m); break;
-            default: ypass_t<GenericDst>(in, out, bs, nbatch, m); break;
+            case 1024: ypass_t<Pow2Dst<1024, T>>(in, out, bs, nbatch, m); break;
+            case 512: ypass_t<Pow2Dst<512, T>>(in, out, bs, nbatch, m); break;
+            case 256: ypass_t<Pow2Dst<256, T>>(in, out, bs, nbatch, m); break;
+            default: ypass_t<GenericDst<T>>(in, out, bs, nbatch, m); break;
         }
         check_launch();
         prof_end(pe, IBPM_KCLASS_YPASS, 16.0 * (double)ng * nbatch);
     }
     // Merged trial solve over all L levels: Gamma_new = Ainv(A Gamma + rest)
     template <class D>
-    void trial_t(const double *Gold, const double *rest_, double *Gnew) {
+    void trial_t(const T *Gold, const T *rest_, T *Gnew) {
         {
             const dim3 grid((ny - 1 + kNG - 1) / kNG, L);
-            const size_t sm = (size_t)(kNG * D::smem_len(plx.M) + D::NWARP * kNG) * sizeof(double2);
+            const size_t sm = pass_smem<D>(plx.M, kNG, kNG);
             const int pe = prof_begin();
             xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1, t2, ng, nx - 1, plx, ny - 1);
             check_launch();
@@ -243,11 +286,11 @@ struct ibpm_handle {
         }
         {
             const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), L);
-            const size_t sm = (size_t)(2 * kNG * D::smem_len(ply.M) + D::NWARP * kNG) * sizeof(double2);
+            const size_t sm = pass_smem<D>(ply.M, 2 * kNG, kNG);
             // the cap must cover the largest M this instantiation serves (kMaxM)
             static bool attr = false;
             if (!attr) {
-                const int cap = (int)((2 * kNG * D::smem_len(kMaxM) + D::NWARP * kNG) * sizeof(double2));
+                const int cap = (int)pass_smem<D>(kMaxM, 2 * kNG, kNG);
                 CK(cudaFuncSetAttribute(ypass_trial_kernel<D, kNG>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
                 attr = true;
             }
@@ -259,15 +302,15 @@ struct ibpm_handle {
         }
         xpass(in_plain(rhs, ng), out_plain(Gnew, ng), L);
     }
-    void trial(const double *Gold, const double *rest_, double *Gnew) {
+    void trial(const T *Gold, const T *rest_, T *Gnew) {
         if (plx.M == 1024 && ply.M == 1024)
-            trial_t<Pow2Dst<1024>>(Gold, rest_, Gnew);
+            trial_t<Pow2Dst<1024, T>>(Gold, rest_, Gnew);
         else if (plx.M == 512 && ply.M == 512)
-            trial_t<Pow2Dst<512>>(Gold, rest_, Gnew);
+            trial_t<Pow2Dst<512, T>>(Gold, rest_, Gnew);
         else if (plx.M == 256 && ply.M == 256)
-            trial_t<Pow2Dst<256>>(Gold, rest_, Gnew);
+            trial_t<Pow2Dst<256, T>>(Gold, rest_, Gnew);
         else
-            trial_t<GenericDst>(Gold, rest_, Gnew);
+            trial_t<GenericDst<T>>(Gold, rest_, Gnew);
     }
 
     Mult mult(int mode, int lev0, int levstep) const {
@@ -283,14 +326,14 @@ struct ibpm_handle {
         m.levstep = levstep;
         return m;
     }
-    InPlain in_plain(const double *p, long long bs) const { return InPlain{p, bs, nx - 1}; }
-    OutPlain out_plain(double *p, long long bs) const { return OutPlain{p, bs, nx - 1}; }
+    InPlain<T> in_plain(const T *p, long long bs) const { return InPlain<T>{p, bs, nx - 1}; }
+    OutPlain<T> out_plain(T *p, long long bs) const { return OutPlain<T>{p, bs, nx - 1}; }
 
     // vort2flux (src/fluid.jl:178-205) over nbatch independent fields.
     // G, psi: level 1 of batch 0, level stride ng, batch stride bs.
     // qout: level 1 of batch 0 (level stride nq, batch stride qbs); curl_all=false
     // computes q only at level 1 (the only level a caller reads).
-    void vort2flux(double *psi_, double *qout, double *Gm, long long bs, long long qbs, int nbatch, bool curl_all) {
+    void vort2flux(T *psi_, T *qout, T *Gm, long long bs, long long qbs, int nbatch, bool curl_all) {
         for (int lev = 2; lev <= L; ++lev) {
             const int nx2 = nx / 2, ny2 = ny / 2;
             const dim3 blk(16, 16), grd((nx2 + 15) / 16, (ny2 + 15) / 16, nbatch);
@@ -298,12 +341,12 @@ struct ibpm_handle {
             check_launch();
         }
         for (int lev = L; lev >= 1; --lev) {
-            double *Gl = Gm + (lev - 1) * ng;
-            double *Pl = psi_ + (lev - 1) * ng;
+            T *Gl = Gm + (lev - 1) * ng;
+            T *Pl = psi_ + (lev - 1) * ng;
             if (lev == L)
                 xpass(in_plain(Gl, bs), out_plain(t1, ng), nbatch);
             else
-                xpass(InBC{Gl, psi_ + lev * ng, bs, bs, g}, out_plain(t1, ng), nbatch);
+                xpass(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, out_plain(t1, ng), nbatch);
             ypass(t1, t2, ng, nbatch, mult(MULT_LAPINV, 1, 0));
             xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch);
             if (curl_all || lev == 1) {
@@ -327,13 +370,13 @@ struct ibpm_handle {
     // B z (src/coupling.jl:163-176) for nbatch vectors z (stride 2np) into x (stride xs).
     void apply_B(const double *z, double *x, long long xs, int nbatch) {
         reg_patch(z, nbatch);
-        InRegRot in{Patch{patch, P.bbox, patch_stride}};
+        InRegRot<T> in{Patch<T>{patch, P.bbox, patch_stride}};
         xpass(in, out_plain(t1, ng), nbatch);
         ypass(t1, t2, ng, nbatch, mult(MULT_AIMPL, 1, 0));
         xpass(in_plain(t2, ng), out_plain(Gw, ng * L), nbatch);
         if (L > 1)
-            CK(cudaMemset2DAsync(Gw + ng, (size_t)(ng * L) * sizeof(double), 0, (size_t)(ng * (L - 1)) * sizeof(double),
-                                 nbatch, st));
+            CK(cudaMemset2DAsync(Gw + ng, (size_t)(ng * L) * sizeof(T), 0, (size_t)(ng * (L - 1)) * sizeof(T), nbatch,
+                                 st));
         vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false);
         launch_regT(P, qw, nq, x, xs, nbatch, 0, prm, g, st);
         check_launch();
@@ -352,6 +395,7 @@ struct ibpm_handle {
 
     // Reads and clears the device error flag; throws on a region error.
     void check_region_error() {
+        cg_collect();
         CK(cudaMemcpyAsync(err_h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         const int e = *err_h;
@@ -366,20 +410,43 @@ struct ibpm_handle {
         }
     }
 
-    static std::string jl_float(double v) {
-        char buf[64];
-        for (int prec = 1; prec <= 17; ++prec) {
-            snprintf(buf, sizeof buf, "%.*g", prec, v);
-            if (strtod(buf, nullptr) == v) break;
-        }
-        std::string s(buf);
-        if (s.find_first_of(".eni") == std::string::npos) s += ".0";
-        return s;
-    }
 
+    // ---- FP32/FP64 conversions for state transfers ----
+    double *staging(size_t n) {
+        if (n > stage_len) {
+            stage = dalloc<double>(n);
+            stage_len = n;
+        }
+        return stage;
+    }
+    void upload(T *dst, const double *src, size_t n);
+    void download(double *dst, const T *src, size_t n);
+
+    void init(const ibpm_problem *p, const ibpm_options &o);
+    ibpm_problem problem_copy{};
+    T *diag_q = nullptr;
+    void set_state(const ibpm_state_view *s) override;
+    void get_state(ibpm_state_view *s) override;
+    bool advance(int64_t nsteps, const ibpm_step_params *params) override;
+    void get_forces(double *fb, double *total) override;
+    void get_time(int64_t *index, double *t) override;
+    void get_info(ibpm_info *info) override;
+    void *stream_ptr() override { return (void *)st; }
+    long long launch_count() const override { return launches; }
+    void set_profile(int enable) override;
+    void read_profile(int kclass, int64_t *launches, double *ms, double *bytes) override;
+    void diag_solve(int op, int level, const double *b, double *x) override;
+    void diag_apply_B(const double *z, double *x) override;
+    void diag_binv(double *out) override;
+    void diag_vort2flux(double *gamma, double *psi, double *q) override;
+    void diag_reg(const double *f, double *gamma1, const double *q1, double *fout) override;
     void setup();
     void build_Binv();
-    int cg(double *x, const double *b);
+    void cg(double *x, const double *b);
+    void cg_collect();
+    int *cg_it = nullptr;
+    bool cg_pending = false, cg_hit_maxiter = false;
+    cudaStream_t st_side = nullptr;
     void step(const ibpm_step_params &prm_in);
     void step_body();
     // CUDA graphs of step_body (static bodies), one per buffer parity
@@ -390,29 +457,31 @@ struct ibpm_handle {
     void materialise_q0();
 };
 
-void ibpm_handle::setup() {
+template <class T>
+void Engine<T>::setup() {
     CK(cudaSetDevice(device));
     if (const char *e = getenv("IBPM_NO_GRAPHS")) use_graphs = e[0] == '0';
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     if (!make_plan(nx, plx) || !make_plan(ny, ply))
         throw ApiError{IBPM_ERR_INVALID, "nx and ny must be even, <= 1024 and of the form 2^a 3^b 5^c"};
     // transform tables
-    auto tables = [&](int M, double2 *&tw, double *&sn, double *&cs, Plan &pl) {
-        std::vector<double2> htw(M);
-        std::vector<double> hsn(M + 1), hcs(M + 1);
+    auto tables = [&](int M, C *&tw, T *&sn, double *&cs, PlanT<T> &pl) {
+        std::vector<C> htw(M);
+        std::vector<T> hsn(M + 1);
+        std::vector<double> hcs(M + 1);
         for (int k = 0; k < M; ++k) {
             const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)M;
-            htw[k] = make_double2((double)cosl(a), (double)sinl(a));
+            htw[k] = Cx<T>::make((T)cosl(a), (T)sinl(a));
         }
         for (int j = 0; j <= M; ++j) {
-            hsn[j] = (double)sinl(3.14159265358979323846264338327950288L * (long double)j / (long double)M);
+            hsn[j] = (T)sinl(3.14159265358979323846264338327950288L * (long double)j / (long double)M);
             hcs[j] = cos(M_PI * j / M);  // _lap_eigs uses cos(pi * i / nx) in Float64
         }
-        tw = dalloc<double2>(M);
-        sn = dalloc<double>(M + 1);
+        tw = dalloc<C>(M);
+        sn = dalloc<T>(M + 1);
         cs = dalloc<double>(M + 1);
-        CK(cudaMemcpyAsync(tw, htw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(sn, hsn.data(), sizeof(double) * (M + 1), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(tw, htw.data(), sizeof(C) * M, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(sn, hsn.data(), sizeof(T) * (M + 1), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(cs, hcs.data(), sizeof(double) * (M + 1), cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));
         pl.tw = tw;
@@ -421,12 +490,12 @@ void ibpm_handle::setup() {
     tables(nx, twx, snx, cx, plx);
     tables(ny, twy, sny, cy, ply);
 
-    q = dalloc<double>(nq * L);
-    psi = dalloc<double>(ng * L);
-    G[0] = dalloc<double>(ng * L);
-    G[1] = dalloc<double>(ng * L);
-    nl[0] = dalloc<double>(ng * L);
-    nl[1] = dalloc<double>(ng * L);
+    q = dalloc<T>(nq * L);
+    psi = dalloc<T>(ng * L);
+    G[0] = dalloc<T>(ng * L);
+    G[1] = dalloc<T>(ng * L);
+    nl[0] = dalloc<T>(ng * L);
+    nl[1] = dalloc<T>(ng * L);
     P.np = np;
     P.xb = dalloc<double>(2 * np);
     P.ub = dalloc<double>(2 * np);
@@ -450,29 +519,31 @@ void ibpm_handle::setup() {
     CK(cudaMemcpyAsync(ref_xb_d, ref_xb.data(), sizeof(double) * 2 * np, cudaMemcpyHostToDevice, st));
 
     // batch width for the B^-1 setup: ~4 GB of column work
-    const long long per_col = (2 * ng * L + nq) * 8 + 2 * ng * 8;
+    const long long per_col = (2 * ng * L + nq + 2 * ng) * (long long)sizeof(T);
     kbatch = (int)std::max(1LL, std::min<long long>(64, (4LL << 30) / per_col));
-    if (!static_bodies) kbatch = 1;
+    if (!static_bodies || !std::is_same<T, double>::value) kbatch = 1;  // FP32 builds B^-1 with an FP64 engine
     kbatch = std::min(kbatch, 2 * np);
     const int kb = std::max(kbatch, L);
-    t1 = dalloc<double>(ng * kb);
-    t2 = dalloc<double>(ng * kb);
-    rhs = dalloc<double>(ng * L);
-    rest = dalloc<double>(ng * L);
-    qs1 = dalloc<double>(nq);
+    t1 = dalloc<T>(ng * kb);
+    t2 = dalloc<T>(ng * kb);
+    rhs = dalloc<T>(ng * L);
+    rest = dalloc<T>(ng * L);
+    qs1 = dalloc<T>(nq);
     Ftmp = dalloc<double>(2 * np);
     const int nchunk = (2 * np + 63) / 64;
     part = dalloc<double>((size_t)nchunk * 2 * np);
     patch_stride = 2LL * (nx + 1) * (ny + 1);
-    patch = dalloc<double>(patch_stride * kbatch);
-    Gw = dalloc<double>(ng * L * kbatch);
-    psiw = dalloc<double>(ng * L * kbatch);
-    qw = dalloc<double>(nq * kbatch);
+    patch = dalloc<T>(patch_stride * kbatch);
+    Gw = dalloc<T>(ng * L * kbatch);
+    psiw = dalloc<T>(ng * L * kbatch);
+    qw = dalloc<T>(nq * kbatch);
     fcol = dalloc<double>(2 * (size_t)np * kbatch);
     cg_u = dalloc<double>(2 * np);
     cg_r = dalloc<double>(2 * np);
     cg_c = dalloc<double>(2 * np);
     cg_s = dalloc<double>(8);
+    cg_it = dalloc<int>(4);
+    CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
 
     // _init_body_motion! (src/bodies.jl:33-41): static bodies take their panels now.
     std::vector<double> hxb(2 * (size_t)np, 0.0), hds(np, 0.0);
@@ -490,13 +561,28 @@ void ibpm_handle::setup() {
     check_region_error();
     if (static_bodies) {
         compute_bbox();
-        build_Binv();
+        if (std::is_same<T, double>::value) {
+            build_Binv();
+        } else {
+            // B and B^-1 in FP64 with a temporary FP64 engine of the same problem;
+            // only the (2np)^2 matrix is kept.
+            Engine<double> e64;
+            ibpm_options o64 = opt;
+            o64.precision = IBPM_FP64;
+            e64.init(&problem_copy, o64);
+            e64.setup();
+            const size_t n = 2 * (size_t)np;
+            Binv = dalloc<double>(n * n);
+            CK(cudaStreamSynchronize(st));
+            CK(cudaMemcpy(Binv, e64.Binv, sizeof(double) * n * n, cudaMemcpyDeviceToDevice));
+        }
     }
     CK(cudaStreamSynchronize(st));
 }
 
 // _Binv_precomputed (src/coupling.jl:187-192): B column by column, then its inverse.
-void ibpm_handle::build_Binv() {
+template <class T>
+void Engine<T>::build_Binv() {
     const int n = 2 * np;
     Binv = dalloc<double>((size_t)n * n);
     rowk = dalloc<double>(n);
@@ -519,91 +605,186 @@ void ibpm_handle::build_Binv() {
 }
 
 namespace {
-// Single-block CG vector kernels (2np is at most a few thousand).
-// mode 0: r = b - c; s[0] = ||r||
-// mode 1: beta = s0^2/s1^2; u = r + beta u
-// mode 2: alpha = s0^2 / dot(u, c); x += alpha u; r -= alpha c; s1 = s0; s0 = ||r||
-__global__ void cg_vec_kernel(int mode, int n, double *x, double *r, double *u, const double *c, const double *b,
-                              double *s) {
+// Device-resident CG state: s[0] = ||r||, s[1] = previous ||r||, s[2] = tol,
+// s[3] = 1 while iterating; it[0] = iterations; err[2] = 1 on a non-finite residual.
+struct CgArgs {
+    int n;
+    double *x, *r, *u, *c;
+    const double *b;
+    double *s;
+    int *it, *err;
+    int maxiter;
+    double reltol, abstol;
+};
+
+__device__ __forceinline__ double cg_block_sum(double v, double *red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+    return t;
+}
+
+// r = b - c (c = B x0); u = 0; residual, tol = max(reltol ||r0||, abstol), and the
+// loop condition of IterativeSolvers' done(): !(it >= maxiter || ||r|| <= tol).
+__global__ void cg_init_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h) {
     __shared__ double red[32];
-    auto block_sum = [&](double v) -> double {
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-        __syncthreads();
-        double t = 0.0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
-        return t;
-    };
-    if (mode == 0) {
-        double a = 0.0;
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            const double v = b[k] - c[k];
-            r[k] = v;
-            u[k] = 0.0;
-            a += v * v;
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < a.n; k += blockDim.x) {
+        const double v = a.b[k] - a.c[k];
+        a.r[k] = v;
+        a.u[k] = 0.0;
+        acc += v * v;
+    }
+    const double t = cg_block_sum(acc, red);
+    if (threadIdx.x == 0) {
+        const double res = sqrt(t);
+        const double tol = fmax(a.reltol * res, a.abstol);
+        int cont = !(0 >= a.maxiter || res <= tol);
+        if (!isfinite(res)) {
+            a.err[2] = 1;
+            cont = 0;
         }
-        const double t = block_sum(a);
-        if (threadIdx.x == 0) {
-            s[0] = sqrt(t);
-            s[1] = 1.0;
+        a.s[0] = res;
+        a.s[1] = 1.0;
+        a.s[2] = tol;
+        a.s[3] = cont;
+        a.it[0] = 0;
+        if (use_h) cudaGraphSetConditional(h, cont ? 1u : 0u);
+    }
+}
+
+// u = r + beta u, beta = ||r||^2 / ||r_prev||^2
+__global__ void cg_dir_kernel(CgArgs a) {
+    const double beta = a.s[0] * a.s[0] / (a.s[1] * a.s[1]);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.n; k += gridDim.x * blockDim.x)
+        a.u[k] = a.r[k] + beta * a.u[k];
+}
+
+// alpha = ||r||^2 / (u . c); x += alpha u; r -= alpha c; new residual and condition
+__global__ void cg_update_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h) {
+    __shared__ double red[32];
+    __shared__ double alpha_s;
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < a.n; k += blockDim.x) acc += a.u[k] * a.c[k];
+    const double uc = cg_block_sum(acc, red);
+    if (threadIdx.x == 0) alpha_s = a.s[0] * a.s[0] / uc;
+    __syncthreads();
+    const double alpha = alpha_s;
+    double rr = 0.0;
+    for (int k = threadIdx.x; k < a.n; k += blockDim.x) {
+        a.x[k] += alpha * a.u[k];
+        const double v = a.r[k] - alpha * a.c[k];
+        a.r[k] = v;
+        rr += v * v;
+    }
+    const double t = cg_block_sum(rr, red);
+    if (threadIdx.x == 0) {
+        const double res = sqrt(t);
+        const int it = a.it[0] + 1;
+        int cont = !(it >= a.maxiter || res <= a.s[2]);
+        if (!isfinite(res)) {
+            a.err[2] = 1;
+            cont = 0;
         }
-    } else if (mode == 1) {
-        const double beta = s[0] * s[0] / (s[1] * s[1]);
-        for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] = r[k] + beta * u[k];
-    } else {
-        double a = 0.0;
-        for (int k = threadIdx.x; k < n; k += blockDim.x) a += u[k] * c[k];
-        const double uc = block_sum(a);
-        const double alpha = s[0] * s[0] / uc;
-        double rr = 0.0;
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            x[k] += alpha * u[k];
-            const double v = r[k] - alpha * c[k];
-            r[k] = v;
-            rr += v * v;
-        }
-        const double t = block_sum(rr);
-        if (threadIdx.x == 0) {
-            s[1] = s[0];
-            s[0] = sqrt(t);
-        }
+        a.s[1] = a.s[0];
+        a.s[0] = res;
+        a.s[3] = cont;
+        a.it[0] = it;
+        if (use_h) cudaGraphSetConditional(h, cont ? 1u : 0u);
     }
 }
 }  // namespace
 
 // IterativeSolvers.jl cg! as called at src/coupling.jl:198-201: plain CG from
 // the initial guess x; stops when ||r|| <= max(reltol ||r0||, abstol) or after
-// maxiter iterations.  Returns the iteration count.
-int ibpm_handle::cg(double *x, const double *b) {
+// maxiter iterations.  All scalars live on the device.  Inside a stream
+// capture the loop is a graph WHILE node whose condition the update kernel
+// sets; otherwise the host reads the condition after every iteration.
+template <class T>
+void Engine<T>::cg(double *x, const double *b) {
     const int n = 2 * np;
+    CgArgs a{n, x, cg_r, cg_u, cg_c, b, cg_s, cg_it, err, opt.cg_maxiter, opt.cg_reltol, opt.cg_abstol};
     apply_B(x, cg_c, n, 1);
-    cg_vec_kernel<<<1, 256, 0, st>>>(0, n, x, cg_r, cg_u, cg_c, b, cg_s);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs == cudaStreamCaptureStatusActive) {
+        cudaGraph_t gr = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &ndeps));
+        cudaGraphConditionalHandle hnd;
+        CK(cudaGraphConditionalHandleCreate(&hnd, gr, 0, 0));
+        cg_init_kernel<<<1, 256, 0, st>>>(a, hnd, 1);
+        check_launch();
+        CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &ndeps));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hnd;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, gr, deps, ndeps, &cp));
+        CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+        // capture the loop body into the WHILE node's graph on the side stream
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        cudaStream_t main = st;
+        st = st_side;
+        try {
+            CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            cg_dir_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
+            check_launch();
+            apply_B(cg_u, cg_c, n, 1);
+            cg_update_kernel<<<1, 256, 0, st>>>(a, hnd, 1);
+            check_launch();
+            cudaGraph_t out = nullptr;
+            CK(cudaStreamEndCapture(st, &out));
+        } catch (...) {
+            cudaGraph_t out = nullptr;
+            cudaStreamEndCapture(st, &out);
+            st = main;
+            throw;
+        }
+        st = main;
+        return;
+    }
+    cg_init_kernel<<<1, 256, 0, st>>>(a, 0, 0);
     check_launch();
-    CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    double res = cg_s_h[0];
-    if (!std::isfinite(res)) throw ApiError{IBPM_ERR_NONFINITE, "non-finite residual in CG"};
-    const double tol = std::max(opt.cg_reltol * res, opt.cg_abstol);
-    int it = 0;
-    while (!(it >= opt.cg_maxiter || res <= tol)) {
-        cg_vec_kernel<<<1, 256, 0, st>>>(1, n, x, cg_r, cg_u, cg_c, b, cg_s);
+    for (;;) {
+        CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (cg_s_h[3] == 0.0) break;
+        cg_dir_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
         check_launch();
         apply_B(cg_u, cg_c, n, 1);
-        cg_vec_kernel<<<1, 256, 0, st>>>(2, n, x, cg_r, cg_u, cg_c, b, cg_s);
+        cg_update_kernel<<<1, 256, 0, st>>>(a, 0, 0);
         check_launch();
-        CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        res = cg_s_h[0];
-        if (!std::isfinite(res)) throw ApiError{IBPM_ERR_NONFINITE, "non-finite residual in CG"};
-        ++it;
     }
-    last_cg_res = res;
-    return it;
+}
+
+// Reads the last step's CG iteration count and residual (after a stream sync).
+template <class T>
+void Engine<T>::cg_collect() {
+    if (!cg_pending) return;
+    CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(err_h + 2, cg_it, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(err_h + 3, err + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cg_pending = false;
+    last_cg_iters = err_h[2];
+    last_cg_res = cg_s_h[0];
+    if (last_cg_iters >= opt.cg_maxiter) cg_hit_maxiter = true;
+    if (err_h[3]) {
+        CK(cudaMemsetAsync(err + 2, 0, sizeof(int), st));
+        throw ApiError{IBPM_ERR_NONFINITE, "non-finite residual in CG"};
+    }
 }
 
 // advance!(::CnabSolver) (src/solver.jl:155-190)
-void ibpm_handle::step(const ibpm_step_params &sp) {
+template <class T>
+void Engine<T>::step(const ibpm_step_params &sp) {
     // inc_time_index! and the host callbacks' values
     ++index;
     prm_h->fs[0] = sp.freestream[0];
@@ -630,9 +811,10 @@ void ibpm_handle::step(const ibpm_step_params &sp) {
     }
     q0_zero = false;
     q0_from_user = false;
-    // Static bodies: the rest of the step is one CUDA graph per parity of the
-    // ping-ponged Gamma / nonlin buffers (gc == nc always), captured on first use.
-    if (static_bodies && use_graphs && !prof) {
+    // The rest of the step is one CUDA graph per parity of the ping-ponged
+    // Gamma / nonlin buffers (gc == nc always), captured on first use; with
+    // moving bodies it holds the CG loop as a WHILE node.
+    if (use_graphs && !prof) {
         const int p = gc;
         if (!graph_exec[p]) {
             const int gc0 = gc, nc0 = nc;
@@ -657,21 +839,23 @@ void ibpm_handle::step(const ibpm_step_params &sp) {
         launches += graph_launches[p];
         gc = 1 - gc;
         nc = 1 - nc;
-        last_cg_iters = 0;
+        if (static_bodies) last_cg_iters = 0;
+        cg_pending = !static_bodies;
         return;
     }
     step_body();
 }
 
 // The device work of one step after the per-step parameters are uploaded.
-void ibpm_handle::step_body() {
+template <class T>
+void Engine<T>::step_body() {
     const long long launches0 = launches;
-    double *Gold = G[gc], *Gnew = G[1 - gc];
-    double *N1 = nl[nc], *N2 = nl[1 - nc];
+    T *Gold = G[gc], *Gnew = G[1 - gc];
+    T *N1 = nl[nc], *N2 = nl[1 - nc];
     // get_trial_state (src/fluid.jl:467-506), all levels at once: the levels
     // only read the previous step's Gamma and q.
     {
-        NonlinArgs a{q, Gold, N1, N2, rest, prm, g};
+        NonlinArgs<T> a{q, Gold, N1, N2, rest, prm, g};
         const dim3 blk(32, 8), grd((nx - 1 + 31) / 32, (ny - 1 + 7) / 8, L);
         const int pe = prof_begin();
         nonlinear_kernel<<<grd, blk, 0, st>>>(a);
@@ -695,15 +879,16 @@ void ibpm_handle::step_body() {
         check_launch();
         last_cg_iters = 0;
     } else {
-        last_cg_iters = cg(Fbt, Ftmp);
+        cg(Fbt, Ftmp);
+        cg_pending = true;
         binv_reduce_kernel<<<1, 1024, 0, st>>>(nullptr, 0, n, Fbt, fb, total, g.h, g.dt, 0);
         check_launch();
     }
     // project_circ (src/coupling.jl:218-230): Gamma = Gamma_s; Gamma_1 -= Ainv_1 rot(E^T F~b)
     reg_patch(Fbt, 1);
-    xpass(InRegRot{Patch{patch, P.bbox, patch_stride}}, out_plain(t1, ng), 1);
+    xpass(InRegRot<T>{Patch<T>{patch, P.bbox, patch_stride}}, out_plain(t1, ng), 1);
     ypass(t1, t2, ng, 1, mult(MULT_AIMPL, 1, 0));
-    xpass(in_plain(t2, ng), OutSub{Gnew, ng, nx - 1}, 1);
+    xpass(in_plain(t2, ng), OutSub<T>{Gnew, ng, nx - 1}, 1);
     // vort2flux!(state.psi, state.q, state.Gamma)
     vort2flux(psi, q, Gnew, 0, 0, 1, true);
     gc = 1 - gc;
@@ -719,7 +904,8 @@ __global__ void eval_prologue_kernel(In in, double *out, int nx, int ny) {
     out[(long long)(i - 1) + (long long)(nx - 1) * (j - 1)] = in(0, i, j);
 }
 
-__global__ void q0_fill_kernel(double *q0, const StepDev *prm, Grid g) {
+template <class T>
+__global__ void q0_fill_kernel(T *q0, const StepDev *prm, Grid g) {
     const long long nu = (long long)(g.nx + 1) * g.ny, nq = nu + (long long)g.nx * (g.ny + 1);
     const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lev = blockIdx.y + 1;
@@ -729,23 +915,271 @@ __global__ void q0_fill_kernel(double *q0, const StepDev *prm, Grid g) {
         v = base_flux_x(g, prm, lev, (int)(f % (g.nx + 1)) + 1, (int)(f / (g.nx + 1)) + 1);
     else
         v = base_flux_y(g, prm, lev, (int)((f - nu) % g.nx) + 1, (int)((f - nu) / g.nx) + 1);
-    q0[(long long)blockIdx.y * nq + f] = v;
+    q0[(long long)blockIdx.y * nq + f] = (T)v;
+}
+
+template <class A, class B>
+__global__ void convert_kernel(B *__restrict__ dst, const A *__restrict__ src, long long n) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        dst[k] = (B)src[k];
 }
 }  // namespace
 
-void ibpm_handle::materialise_q0() {
-    if (!q0mat) q0mat = dalloc<double>(nq * L);
+template <class T>
+void Engine<T>::upload(T *dst, const double *src, size_t n) {
+    if (std::is_same<T, double>::value) {
+        CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        return;
+    }
+    double *tmp = staging(n);
+    CK(cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    convert_kernel<double, T><<<1184, 256, 0, st>>>(dst, tmp, (long long)n);
+    check_launch();
+}
+
+template <class T>
+void Engine<T>::download(double *dst, const T *src, size_t n) {
+    if (std::is_same<T, double>::value) {
+        CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        return;
+    }
+    double *tmp = staging(n);
+    convert_kernel<T, double><<<1184, 256, 0, st>>>(tmp, src, (long long)n);
+    check_launch();
+    CK(cudaMemcpyAsync(dst, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+void Engine<T>::materialise_q0() {
+    if (!q0mat) q0mat = dalloc<T>(nq * L);
     if (q0_from_user) return;
     if (q0_zero) {
-        CK(cudaMemsetAsync(q0mat, 0, sizeof(double) * nq * L, st));
+        CK(cudaMemsetAsync(q0mat, 0, sizeof(T) * nq * L, st));
         return;
     }
     prm_h->fs[0] = fs_last[0];
     prm_h->fs[1] = fs_last[1];
     for (int k = 0; k < 6; ++k) prm_h->gm[k] = gm_last[k];
     CK(cudaMemcpyAsync(prm, prm_h, sizeof(StepDev), cudaMemcpyHostToDevice, st));
-    q0_fill_kernel<<<dim3((unsigned)((nq + 255) / 256), L), 256, 0, st>>>(q0mat, prm, g);
+    q0_fill_kernel<T><<<dim3((unsigned)((nq + 255) / 256), L), 256, 0, st>>>(q0mat, prm, g);
     check_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Engine methods behind the C ABI
+// ---------------------------------------------------------------------------
+
+template <class T>
+void Engine<T>::init(const ibpm_problem *p, const ibpm_options &o) {
+    opt = o;
+    device = o.device;
+    nx = p->nx;
+    ny = p->ny;
+    L = p->nlevel;
+    np = p->npanel;
+    nbody = p->nbody;
+    nu = (long long)(p->nx + 1) * p->ny;
+    nq = nu + (long long)p->nx * (p->ny + 1);
+    ng = (long long)(p->nx - 1) * (p->ny - 1);
+    nbc = 2LL * (p->nx + 1) + 2LL * (p->ny + 1);
+    g = Grid{p->nx, p->ny, p->nlevel, p->h, p->x0, p->y0, p->Re, p->dt, p->grid_moving ? 1 : 0};
+    body_kind.assign(p->body_kind, p->body_kind + p->nbody);
+    body_start.assign(p->body_start, p->body_start + p->nbody + 1);
+    ref_xb.assign(p->body_xb, p->body_xb + 2 * (size_t)p->npanel);
+    ref_ds.assign(p->body_ds, p->body_ds + p->npanel);
+    static_bodies = true;
+    for (int b = 0; b < p->nbody; ++b)
+        if (body_kind[b] != IBPM_BODY_STATIC) static_bodies = false;
+    problem_copy = *p;
+    problem_copy.body_kind = body_kind.data();
+    problem_copy.body_start = body_start.data();
+    problem_copy.body_xb = ref_xb.data();
+    problem_copy.body_ds = ref_ds.data();
+}
+
+template <class T>
+void Engine<T>::set_state(const ibpm_state_view *s) {
+    CK(cudaSetDevice(device));
+    const size_t ngL = (size_t)(ng * L), nqL = (size_t)(nq * L);
+    const size_t np2 = sizeof(double) * 2 * np;
+    index = s->index;
+    t0 = s->t0;
+    if (s->q) upload(q, s->q, nqL);
+    if (s->q0) {
+        if (!q0mat) q0mat = dalloc<T>(nq * L);
+        upload(q0mat, s->q0, nqL);
+        q0_from_user = true;
+    }
+    if (s->gamma) upload(G[gc], s->gamma, ngL);
+    if (s->psi) upload(psi, s->psi, ngL);
+    if (s->nonlin1) upload(nl[nc], s->nonlin1, ngL);
+    if (s->nonlin2) upload(nl[1 - nc], s->nonlin2, ngL);
+    if (s->xb) CK(cudaMemcpyAsync(P.xb, s->xb, np2, cudaMemcpyHostToDevice, st));
+    if (s->ds) CK(cudaMemcpyAsync(ds, s->ds, np2 / 2, cudaMemcpyHostToDevice, st));
+    if (s->ub) CK(cudaMemcpyAsync(P.ub, s->ub, np2, cudaMemcpyHostToDevice, st));
+    if (s->fbt) CK(cudaMemcpyAsync(Fbt, s->fbt, np2, cudaMemcpyHostToDevice, st));
+    fs_last[0] = s->freestream[0];
+    fs_last[1] = s->freestream[1];
+    // update_vars! (problem.jl:676-685)
+    binv_reduce_kernel<<<1, 1024, 0, st>>>(nullptr, 0, 2 * np, Fbt, fb, total, g.h, g.dt, 0);
+    check_launch();
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+void Engine<T>::get_state(ibpm_state_view *s) {
+    CK(cudaSetDevice(device));
+    const size_t ngL = (size_t)(ng * L), nqL = (size_t)(nq * L);
+    const size_t np2 = sizeof(double) * 2 * np;
+    s->index = index;
+    s->t0 = t0;
+    s->freestream[0] = fs_last[0];
+    s->freestream[1] = fs_last[1];
+    if (s->q) download(s->q, q, nqL);
+    if (s->q0) {
+        materialise_q0();
+        download(s->q0, q0mat, nqL);
+    }
+    if (s->gamma) download(s->gamma, G[gc], ngL);
+    if (s->psi) download(s->psi, psi, ngL);
+    if (s->nonlin1) download(s->nonlin1, nl[nc], ngL);
+    if (s->nonlin2) download(s->nonlin2, nl[1 - nc], ngL);
+    if (s->xb) CK(cudaMemcpyAsync(s->xb, P.xb, np2, cudaMemcpyDeviceToHost, st));
+    if (s->ds) CK(cudaMemcpyAsync(s->ds, ds, np2 / 2, cudaMemcpyDeviceToHost, st));
+    if (s->ub) CK(cudaMemcpyAsync(s->ub, P.ub, np2, cudaMemcpyDeviceToHost, st));
+    if (s->fbt) CK(cudaMemcpyAsync(s->fbt, Fbt, np2, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+bool Engine<T>::advance(int64_t nsteps, const ibpm_step_params *params) {
+    CK(cudaSetDevice(device));
+    cg_hit_maxiter = false;
+    for (int64_t k = 0; k < nsteps; ++k) step(params[k]);
+    CK(cudaStreamSynchronize(st));
+    cg_collect();
+    return cg_hit_maxiter;
+}
+
+template <class T>
+void Engine<T>::get_forces(double *fbo, double *tot) {
+    CK(cudaSetDevice(device));
+    if (fbo) CK(cudaMemcpyAsync(fbo, fb, sizeof(double) * 2 * np, cudaMemcpyDeviceToHost, st));
+    if (tot) CK(cudaMemcpyAsync(tot, total, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+void Engine<T>::get_time(int64_t *idx, double *t) {
+    if (idx) *idx = index;
+    if (t) *t = t0 + g.dt * (double)(index - 1);
+}
+
+template <class T>
+void Engine<T>::get_info(ibpm_info *info) {
+    info->nq = nq;
+    info->ng = ng;
+    info->nbc = nbc;
+    info->static_bodies = static_bodies ? 1 : 0;
+    info->last_cg_iters = last_cg_iters;
+    info->last_cg_residual = last_cg_res;
+    info->device_bytes = dev_bytes;
+}
+
+template <class T>
+void Engine<T>::set_profile(int enable) {
+    CK(cudaStreamSynchronize(st));
+    prof = enable != 0;
+    prof_recs.clear();
+    ev_next = 0;
+}
+
+template <class T>
+void Engine<T>::read_profile(int kclass, int64_t *launches_out, double *ms, double *bytes) {
+    CK(cudaStreamSynchronize(st));
+    int64_t n = 0;
+    double t = 0.0, b = 0.0;
+    for (const auto &r : prof_recs) {
+        if (r.cls != kclass) continue;
+        float e = 0.f;
+        CK(cudaEventElapsedTime(&e, ev_pool[r.ev], ev_pool[r.ev + 1]));
+        ++n;
+        t += e;
+        b += r.bytes;
+    }
+    if (launches_out) *launches_out = n;
+    if (ms) *ms = t;
+    if (bytes) *bytes = b;
+}
+
+template <class T>
+void Engine<T>::diag_solve(int op, int level, const double *b, double *x) {
+    if (op < 0 || op > 2 || level < 1 || level > L) throw ApiError{IBPM_ERR_INVALID, "bad diag_solve arguments"};
+    CK(cudaSetDevice(device));
+    upload(rhs, b, (size_t)ng);
+    const int mode = op == 0 ? MULT_LAPINV : (op == 1 ? MULT_AEXPL : MULT_AIMPL);
+    xpass(in_plain(rhs, ng), out_plain(t1, ng), 1);
+    ypass(t1, t2, ng, 1, mult(mode, level, 0));
+    xpass(in_plain(t2, ng), out_plain(rhs, ng), 1);
+    download(x, rhs, (size_t)ng);
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+void Engine<T>::diag_apply_B(const double *z, double *x) {
+    CK(cudaSetDevice(device));
+    const size_t bytes = sizeof(double) * 2 * np;
+    CK(cudaMemcpyAsync(cg_u, z, bytes, cudaMemcpyHostToDevice, st));
+    compute_bbox();
+    apply_B(cg_u, cg_c, 2 * np, 1);
+    CK(cudaMemcpyAsync(x, cg_c, bytes, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+void Engine<T>::diag_binv(double *out) {
+    if (!Binv) throw ApiError{IBPM_ERR_INVALID, "no precomputed B^-1 (moving bodies)"};
+    const size_t n = 2 * (size_t)np;
+    CK(cudaMemcpyAsync(out, Binv, sizeof(double) * n * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+void Engine<T>::diag_vort2flux(double *gamma, double *psi_out, double *q_out) {
+    CK(cudaSetDevice(device));
+    const size_t ngL = (size_t)(ng * L);
+    upload(Gw, gamma, ngL);
+    if (!diag_q) diag_q = dalloc<T>(nq * L);
+    vort2flux(psiw, diag_q, Gw, 0, 0, 1, true);
+    download(gamma, Gw, ngL);
+    download(psi_out, psiw, ngL);
+    download(q_out, diag_q, (size_t)(nq * L));
+    CK(cudaStreamSynchronize(st));
+}
+
+template <class T>
+void Engine<T>::diag_reg(const double *f, double *gamma1, const double *q1, double *fout) {
+    CK(cudaSetDevice(device));
+    const size_t nf = sizeof(double) * 2 * np;
+    compute_bbox();
+    if (f && gamma1) {
+        CK(cudaMemcpyAsync(cg_u, f, nf, cudaMemcpyHostToDevice, st));
+        reg_patch(cg_u, 1);
+        double *out = staging((size_t)ng);
+        const dim3 blk(32, 8), grd((nx - 1 + 31) / 32, (ny - 1 + 7) / 8);
+        eval_prologue_kernel<<<grd, blk, 0, st>>>(InRegRot<T>{Patch<T>{patch, P.bbox, patch_stride}}, out, nx, ny);
+        check_launch();
+        CK(cudaMemcpyAsync(gamma1, out, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    if (q1 && fout) {
+        upload(qw, q1, (size_t)nq);
+        launch_regT(P, qw, 0, cg_c, 0, 1, 0, prm, g, st);
+        check_launch();
+        CK(cudaMemcpyAsync(fout, cg_c, nf, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
 }
 
 // ---------------------------------------------------------------------------
@@ -769,6 +1203,20 @@ static int guarded(ibpm_handle *h, F &&f) {
     }
 }
 
+template <class T>
+static int create_engine(const ibpm_problem *p, const ibpm_options &opt, ibpm_handle **out) {
+    Engine<T> *h = new Engine<T>();
+    h->init(p, opt);
+    const int rc = guarded(h, [&] { h->setup(); });
+    if (rc != IBPM_OK) {
+        g_create_error = h->last_error;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return IBPM_OK;
+}
+
 extern "C" {
 
 void ibpm_default_options(ibpm_options *opt) {
@@ -789,7 +1237,7 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
     ibpm_options opt;
     ibpm_default_options(&opt);
     if (opt_in) opt = *opt_in;
-    if (opt.precision != IBPM_FP64) {
+    if (opt.precision != IBPM_FP64 && opt.precision != IBPM_FP32) {
         g_create_error = "unsupported precision mode";
         return IBPM_ERR_INVALID;
     }
@@ -802,133 +1250,51 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
         g_create_error = "body_start must run from 0 to npanel";
         return IBPM_ERR_INVALID;
     }
+    for (int b = 0; b < p->nbody; ++b)
+        if (p->body_kind[b] != IBPM_BODY_STATIC && p->body_kind[b] != IBPM_BODY_MOVING_RIGID) {
+            g_create_error = "unknown body kind";
+            return IBPM_ERR_INVALID;
+        }
+    // The reference rejects out-of-region static panels while building the
+    // Regularization (coupling.jl:38-41), before any size restriction of ours.
+    for (int b = 0; b < p->nbody; ++b) {
+        if (p->body_kind[b] != IBPM_BODY_STATIC) continue;
+        for (int k = p->body_start[b]; k < p->body_start[b + 1]; ++k) {
+            const double xb = p->body_xb[k], yb = p->body_xb[p->npanel + k];
+            const int ix = (int)nearbyint((xb - p->x0) / p->h + 1.0 - 0.25);
+            const int iy = (int)nearbyint((yb - p->y0) / p->h + 1.0 - 0.25);
+            if (!(3 < ix && ix <= p->nx - 3) || !(3 < iy && iy <= p->ny - 3)) {
+                g_create_error = "Panel index=" + std::to_string(k + 1) + " at (" + jl_float(xb) + ", " +
+                                 jl_float(yb) + ") outside allowed region";
+                return IBPM_ERR_REGION;
+            }
+        }
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= opt.device) {
         g_create_error = "no CUDA device available";
         return IBPM_ERR_CUDA;
     }
-    ibpm_handle *h = new ibpm_handle();
-    h->opt = opt;
-    h->device = opt.device;
-    h->nx = p->nx;
-    h->ny = p->ny;
-    h->L = p->nlevel;
-    h->np = p->npanel;
-    h->nbody = p->nbody;
-    h->nu = (long long)(p->nx + 1) * p->ny;
-    h->nq = h->nu + (long long)p->nx * (p->ny + 1);
-    h->ng = (long long)(p->nx - 1) * (p->ny - 1);
-    h->nbc = 2LL * (p->nx + 1) + 2LL * (p->ny + 1);
-    h->g = Grid{p->nx, p->ny, p->nlevel, p->h, p->x0, p->y0, p->Re, p->dt, p->grid_moving ? 1 : 0};
-    h->body_kind.assign(p->body_kind, p->body_kind + p->nbody);
-    h->body_start.assign(p->body_start, p->body_start + p->nbody + 1);
-    h->ref_xb.assign(p->body_xb, p->body_xb + 2 * (size_t)p->npanel);
-    h->ref_ds.assign(p->body_ds, p->body_ds + p->npanel);
-    for (int b = 0; b < p->nbody; ++b) {
-        if (h->body_kind[b] != IBPM_BODY_STATIC && h->body_kind[b] != IBPM_BODY_MOVING_RIGID) {
-            g_create_error = "unknown body kind";
-            delete h;
-            return IBPM_ERR_INVALID;
-        }
-        if (h->body_kind[b] != IBPM_BODY_STATIC) h->static_bodies = false;
-    }
-    // The reference rejects out-of-region static panels while building the
-    // Regularization (coupling.jl:38-41), before any size restriction of ours.
-    for (int b = 0; b < p->nbody; ++b) {
-        if (h->body_kind[b] != IBPM_BODY_STATIC) continue;
-        for (int k = h->body_start[b]; k < h->body_start[b + 1]; ++k) {
-            const double xb = h->ref_xb[k], yb = h->ref_xb[p->npanel + k];
-            const int ix = (int)nearbyint((xb - p->x0) / p->h + 1.0 - 0.25);
-            const int iy = (int)nearbyint((yb - p->y0) / p->h + 1.0 - 0.25);
-            if (!(3 < ix && ix <= p->nx - 3) || !(3 < iy && iy <= p->ny - 3)) {
-                g_create_error = "Panel index=" + std::to_string(k + 1) + " at (" + ibpm_handle::jl_float(xb) + ", " +
-                                 ibpm_handle::jl_float(yb) + ") outside allowed region";
-                delete h;
-                return IBPM_ERR_REGION;
-            }
-        }
-    }
-    const int rc = guarded(h, [&] { h->setup(); });
-    if (rc != IBPM_OK) {
-        g_create_error = h->last_error;
-        delete h;
-        return rc;
-    }
-    *out = h;
-    return IBPM_OK;
+    if (opt.precision == IBPM_FP32) return create_engine<float>(p, opt, out);
+    return create_engine<double>(p, opt, out);
 }
 
 void ibpm_destroy(ibpm_handle *h) { delete h; }
 
 int ibpm_set_state(ibpm_handle *h, const ibpm_state_view *s) {
     if (!h || !s) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        const size_t ngL = sizeof(double) * h->ng * h->L, nqL = sizeof(double) * h->nq * h->L;
-        const size_t np2 = sizeof(double) * 2 * h->np;
-        h->index = s->index;
-        h->t0 = s->t0;
-        if (s->q) CK(cudaMemcpyAsync(h->q, s->q, nqL, cudaMemcpyHostToDevice, h->st));
-        if (s->q0) {
-            if (!h->q0mat) h->q0mat = h->dalloc<double>(h->nq * h->L);
-            CK(cudaMemcpyAsync(h->q0mat, s->q0, nqL, cudaMemcpyHostToDevice, h->st));
-            h->q0_from_user = true;
-        }
-        if (s->gamma) CK(cudaMemcpyAsync(h->G[h->gc], s->gamma, ngL, cudaMemcpyHostToDevice, h->st));
-        if (s->psi) CK(cudaMemcpyAsync(h->psi, s->psi, ngL, cudaMemcpyHostToDevice, h->st));
-        if (s->nonlin1) CK(cudaMemcpyAsync(h->nl[h->nc], s->nonlin1, ngL, cudaMemcpyHostToDevice, h->st));
-        if (s->nonlin2) CK(cudaMemcpyAsync(h->nl[1 - h->nc], s->nonlin2, ngL, cudaMemcpyHostToDevice, h->st));
-        if (s->xb) CK(cudaMemcpyAsync(h->P.xb, s->xb, np2, cudaMemcpyHostToDevice, h->st));
-        if (s->ds) CK(cudaMemcpyAsync(h->ds, s->ds, np2 / 2, cudaMemcpyHostToDevice, h->st));
-        if (s->ub) CK(cudaMemcpyAsync(h->P.ub, s->ub, np2, cudaMemcpyHostToDevice, h->st));
-        if (s->fbt) CK(cudaMemcpyAsync(h->Fbt, s->fbt, np2, cudaMemcpyHostToDevice, h->st));
-        h->fs_last[0] = s->freestream[0];
-        h->fs_last[1] = s->freestream[1];
-        // update_vars! (problem.jl:676-685)
-        binv_reduce_kernel<<<1, 1024, 0, h->st>>>(nullptr, 0, 2 * h->np, h->Fbt, h->fb, h->total, h->g.h, h->g.dt, 0);
-        h->check_launch();
-        CK(cudaStreamSynchronize(h->st));
-    });
+    return guarded(h, [&] { h->set_state(s); });
 }
 
 int ibpm_get_state(ibpm_handle *h, ibpm_state_view *s) {
     if (!h || !s) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        const size_t ngL = sizeof(double) * h->ng * h->L, nqL = sizeof(double) * h->nq * h->L;
-        const size_t np2 = sizeof(double) * 2 * h->np;
-        s->index = h->index;
-        s->t0 = h->t0;
-        s->freestream[0] = h->fs_last[0];
-        s->freestream[1] = h->fs_last[1];
-        if (s->q) CK(cudaMemcpyAsync(s->q, h->q, nqL, cudaMemcpyDeviceToHost, h->st));
-        if (s->q0) {
-            h->materialise_q0();
-            CK(cudaMemcpyAsync(s->q0, h->q0mat, nqL, cudaMemcpyDeviceToHost, h->st));
-        }
-        if (s->gamma) CK(cudaMemcpyAsync(s->gamma, h->G[h->gc], ngL, cudaMemcpyDeviceToHost, h->st));
-        if (s->psi) CK(cudaMemcpyAsync(s->psi, h->psi, ngL, cudaMemcpyDeviceToHost, h->st));
-        if (s->nonlin1) CK(cudaMemcpyAsync(s->nonlin1, h->nl[h->nc], ngL, cudaMemcpyDeviceToHost, h->st));
-        if (s->nonlin2) CK(cudaMemcpyAsync(s->nonlin2, h->nl[1 - h->nc], ngL, cudaMemcpyDeviceToHost, h->st));
-        if (s->xb) CK(cudaMemcpyAsync(s->xb, h->P.xb, np2, cudaMemcpyDeviceToHost, h->st));
-        if (s->ds) CK(cudaMemcpyAsync(s->ds, h->ds, np2 / 2, cudaMemcpyDeviceToHost, h->st));
-        if (s->ub) CK(cudaMemcpyAsync(s->ub, h->P.ub, np2, cudaMemcpyDeviceToHost, h->st));
-        if (s->fbt) CK(cudaMemcpyAsync(s->fbt, h->Fbt, np2, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-    });
+    return guarded(h, [&] { h->get_state(s); });
 }
 
 int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params) {
     if (!h || nsteps < 0 || (nsteps > 0 && !params)) return IBPM_ERR_INVALID;
     bool maxiter = false;
-    const int rc = guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        for (int64_t k = 0; k < nsteps; ++k) {
-            h->step(params[k]);
-            if (!h->static_bodies && h->last_cg_iters >= h->opt.cg_maxiter) maxiter = true;
-        }
-        CK(cudaStreamSynchronize(h->st));
-    });
+    const int rc = guarded(h, [&] { maxiter = h->advance(nsteps, params); });
     if (rc != IBPM_OK) return rc;
     if (maxiter) {
         h->last_error = "CG reached maxiter";
@@ -939,149 +1305,60 @@ int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params)
 
 int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force) {
     if (!h) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        if (fb) CK(cudaMemcpyAsync(fb, h->fb, sizeof(double) * 2 * h->np, cudaMemcpyDeviceToHost, h->st));
-        if (total_force) CK(cudaMemcpyAsync(total_force, h->total, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-    });
+    return guarded(h, [&] { h->get_forces(fb, total_force); });
 }
 
 int ibpm_get_time(ibpm_handle *h, int64_t *index, double *t) {
     if (!h) return IBPM_ERR_INVALID;
-    if (index) *index = h->index;
-    if (t) *t = h->t0 + h->g.dt * (double)(h->index - 1);
+    h->get_time(index, t);
     return IBPM_OK;
 }
 
 int ibpm_get_info(ibpm_handle *h, ibpm_info *info) {
     if (!h || !info) return IBPM_ERR_INVALID;
-    info->nq = h->nq;
-    info->ng = h->ng;
-    info->nbc = h->nbc;
-    info->static_bodies = h->static_bodies ? 1 : 0;
-    info->last_cg_iters = h->last_cg_iters;
-    info->last_cg_residual = h->last_cg_res;
-    info->device_bytes = h->dev_bytes;
+    h->get_info(info);
     return IBPM_OK;
 }
 
 const char *ibpm_last_error(const ibpm_handle *h) { return h ? h->last_error.c_str() : g_create_error.c_str(); }
 
-void *ibpm_stream(ibpm_handle *h) { return h ? (void *)h->st : nullptr; }
+void *ibpm_stream(ibpm_handle *h) { return h ? h->stream_ptr() : nullptr; }
 
-int64_t ibpm_kernel_launches(const ibpm_handle *h) { return h ? h->launches : 0; }
+int64_t ibpm_kernel_launches(const ibpm_handle *h) { return h ? h->launch_count() : 0; }
 
 int ibpm_diag_solve(ibpm_handle *h, int op, int level, const double *b, double *x) {
-    if (!h || !b || !x || op < 0 || op > 2 || level < 1 || level > h->L) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        const size_t bytes = sizeof(double) * h->ng;
-        CK(cudaMemcpyAsync(h->rhs, b, bytes, cudaMemcpyHostToDevice, h->st));
-        const int mode = op == 0 ? MULT_LAPINV : (op == 1 ? MULT_AEXPL : MULT_AIMPL);
-        h->xpass(h->in_plain(h->rhs, h->ng), h->out_plain(h->t1, h->ng), 1);
-        h->ypass(h->t1, h->t2, h->ng, 1, h->mult(mode, level, 0));
-        h->xpass(h->in_plain(h->t2, h->ng), h->out_plain(h->rhs, h->ng), 1);
-        CK(cudaMemcpyAsync(x, h->rhs, bytes, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-    });
+    if (!h || !b || !x) return IBPM_ERR_INVALID;
+    return guarded(h, [&] { h->diag_solve(op, level, b, x); });
 }
 
 int ibpm_diag_apply_B(ibpm_handle *h, const double *z, double *x) {
     if (!h || !z || !x) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        const size_t bytes = sizeof(double) * 2 * h->np;
-        CK(cudaMemcpyAsync(h->cg_u, z, bytes, cudaMemcpyHostToDevice, h->st));
-        h->compute_bbox();
-        h->apply_B(h->cg_u, h->cg_c, 2 * h->np, 1);
-        CK(cudaMemcpyAsync(x, h->cg_c, bytes, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-    });
+    return guarded(h, [&] { h->diag_apply_B(z, x); });
 }
 
 int ibpm_diag_binv(ibpm_handle *h, double *out) {
     if (!h || !out) return IBPM_ERR_INVALID;
-    if (!h->Binv) {
-        h->last_error = "no precomputed B^-1 (moving bodies)";
-        return IBPM_ERR_INVALID;
-    }
-    return guarded(h, [&] {
-        const size_t n = 2 * (size_t)h->np;
-        CK(cudaMemcpyAsync(out, h->Binv, sizeof(double) * n * n, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-    });
+    return guarded(h, [&] { h->diag_binv(out); });
 }
 
 int ibpm_diag_vort2flux(ibpm_handle *h, double *gamma, double *psi, double *q) {
     if (!h || !gamma || !psi || !q) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        const size_t ngL = sizeof(double) * h->ng * h->L;
-        CK(cudaMemcpyAsync(h->Gw, gamma, ngL, cudaMemcpyHostToDevice, h->st));
-        double *qd = h->dalloc<double>(h->nq * h->L);
-        h->vort2flux(h->psiw, qd, h->Gw, 0, 0, 1, true);
-        CK(cudaMemcpyAsync(gamma, h->Gw, ngL, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaMemcpyAsync(psi, h->psiw, ngL, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaMemcpyAsync(q, qd, sizeof(double) * h->nq * h->L, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-    });
+    return guarded(h, [&] { h->diag_vort2flux(gamma, psi, q); });
 }
 
 int ibpm_diag_reg(ibpm_handle *h, const double *f, double *gamma1, const double *q1, double *fout) {
     if (!h) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaSetDevice(h->device));
-        const size_t nf = sizeof(double) * 2 * h->np;
-        h->compute_bbox();
-        if (f && gamma1) {
-            CK(cudaMemcpyAsync(h->cg_u, f, nf, cudaMemcpyHostToDevice, h->st));
-            h->reg_patch(h->cg_u, 1);
-            // the X-pass prologue (InRegRot) evaluated on every Gamma point
-            const dim3 blk(32, 8), grd((h->nx - 1 + 31) / 32, (h->ny - 1 + 7) / 8);
-            eval_prologue_kernel<<<grd, blk, 0, h->st>>>(InRegRot{Patch{h->patch, h->P.bbox, h->patch_stride}}, h->t2,
-                                                         h->nx, h->ny);
-            h->check_launch();
-            CK(cudaMemcpyAsync(gamma1, h->t2, sizeof(double) * h->ng, cudaMemcpyDeviceToHost, h->st));
-        }
-        if (q1 && fout) {
-            CK(cudaMemcpyAsync(h->qw, q1, sizeof(double) * h->nq, cudaMemcpyHostToDevice, h->st));
-            launch_regT(h->P, h->qw, 0, h->cg_c, 0, 1, 0, h->prm, h->g, h->st);
-            h->check_launch();
-            CK(cudaMemcpyAsync(fout, h->cg_c, nf, cudaMemcpyDeviceToHost, h->st));
-        }
-        CK(cudaStreamSynchronize(h->st));
-    });
+    return guarded(h, [&] { h->diag_reg(f, gamma1, q1, fout); });
 }
 
 int ibpm_profile(ibpm_handle *h, int enable) {
     if (!h) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaStreamSynchronize(h->st));
-        h->prof = enable != 0;
-        h->prof_recs.clear();
-        h->ev_next = 0;
-    });
+    return guarded(h, [&] { h->set_profile(enable); });
 }
 
 int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms, double *bytes) {
     if (!h || kclass < 0 || kclass >= IBPM_KCLASS_COUNT) return IBPM_ERR_INVALID;
-    return guarded(h, [&] {
-        CK(cudaStreamSynchronize(h->st));
-        int64_t n = 0;
-        double t = 0.0, b = 0.0;
-        for (const auto &r : h->prof_recs) {
-            if (r.cls != kclass) continue;
-            float e = 0.f;
-            CK(cudaEventElapsedTime(&e, h->ev_pool[r.ev], h->ev_pool[r.ev + 1]));
-            ++n;
-            t += e;
-            b += r.bytes;
-        }
-        if (launches) *launches = n;
-        if (ms) *ms = t;
-        if (bytes) *bytes = b;
-    });
+    return guarded(h, [&] { h->read_profile(kclass, launches, ms, bytes); });
 }
 
 }  // extern "C"

@@ -1,5 +1,7 @@
-// kernels.cuh -- FP64 device kernels of the IBPM time step (line passes,
-// stencils, B^-1 algebra).  Included by ibpm.cu only.
+// kernels.cuh -- device kernels of the IBPM time step (line passes, stencils,
+// B^-1 algebra).  Field element type T is double (plain FP64 path) or float
+// (mixed-precision path); arithmetic on boundary values, multipliers and
+// coupling sums is done in double.  Included by ibpm.cu only.
 #pragma once
 #include "common.cuh"
 #include "fft_pow2.cuh"
@@ -10,26 +12,39 @@ namespace ibpm {
 // Line-pass kernels
 // ---------------------------------------------------------------------------
 
+// Shared-memory layout of a pass kernel: nbuf line buffers of D::C, then the
+// double2 scan scratch at a 16-byte boundary.
+template <class D>
+__host__ __device__ constexpr size_t scratch_offset(int M, int nbuf) {
+    return ((size_t)nbuf * D::smem_len(M) * sizeof(typename D::C) + 15) / 16 * 16;
+}
+template <class D>
+__host__ __device__ constexpr size_t pass_smem(int M, int nbuf, int ngroups) {
+    return scratch_offset<D>(M, nbuf) + (size_t)D::NWARP * ngroups * sizeof(double2);
+}
+
 // Prologue: plain field
+template <class T>
 struct InPlain {
-    const double *p;
+    const T *p;
     long long bs;
     int ld;
     __device__ __forceinline__ double operator()(int b, int i, int j) const {
-        return p[b * bs + (long long)(i - 1) + (long long)ld * (j - 1)];
+        return (double)p[b * bs + (long long)(i - 1) + (long long)ld * (j - 1)];
     }
 };
 
 // Prologue of vort2flux's telescoping solve (src/fluid.jl:194-197):
 // Gamma_tmp = Gamma[:, lev]; apply_bc!(Gamma_tmp, get_bc(psi[:, lev+1]); fac=1)
+template <class T>
 struct InBC {
-    const double *gam;
-    const double *coarse;
+    const T *gam;
+    const T *coarse;
     long long bs, cbs;
     Grid g;
     __device__ __forceinline__ double operator()(int b, int i, int j) const {
-        const double *G = gam + b * bs;
-        double v = G[GI(i, j)];
+        const T *G = gam + b * bs;
+        double v = (double)G[GI(i, j)];
         if (on_ring(g, i, j)) v = apply_bc_at(v, coarse + b * cbs, g, i, j, 1.0);
         return v;
     }
@@ -37,53 +52,34 @@ struct InBC {
 
 // Prologue rot!(Gamma, reg!(q, f)) (src/fluid.jl:101-111 after src/coupling.jl:72-85),
 // evaluated from the regularised patch.
+template <class T>
 struct InRegRot {
-    Patch pt;
+    Patch<T> pt;
     __device__ __forceinline__ double operator()(int b, int I, int J) const {
         return (pt.get(b, 0, I + 1, J) - pt.get(b, 0, I + 1, J + 1)) + (pt.get(b, 1, I + 1, J + 1) - pt.get(b, 1, I, J + 1));
     }
 };
 
 // Epilogue: plain store
+template <class T>
 struct OutPlain {
-    double *p;
+    T *p;
     long long bs;
     int ld;
     __device__ __forceinline__ void operator()(int b, int i, int j, double v) const {
-        p[b * bs + (long long)(i - 1) + (long long)ld * (j - 1)] = v;
+        p[b * bs + (long long)(i - 1) + (long long)ld * (j - 1)] = (T)v;
     }
 };
 
 // Epilogue of project_circ (src/coupling.jl:227): Gamma[:, 1] .-= x
+template <class T>
 struct OutSub {
-    double *p;
+    T *p;
     long long bs;
     int ld;
     __device__ __forceinline__ void operator()(int b, int i, int j, double v) const {
-        double *q = p + b * bs + (long long)(i - 1) + (long long)ld * (j - 1);
-        *q = *q - v;
-    }
-};
-
-// Epilogue of rhs = A Gamma in get_trial_state (src/fluid.jl:485-493):
-// rhs = ((A Gamma + dt b1 N1) + dt b2 N2) + rhsbc, rhsbc = apply_bc!(0, get_bc(Gamma[:, lev+1]); fac)
-struct OutTrialRhs {
-    double *rhs;
-    const double *n1, *n2;
-    const double *gam_old;  // Gamma at all levels (level stride bs)
-    long long bs;
-    Grid g;
-    __device__ __forceinline__ void operator()(int b, int i, int j, double v) const {
-        const int lev = b + 1;
-        const long long k = b * bs + GI(i, j);
-        const double f1 = g.dt * 1.5, f2 = g.dt * -0.5;
-        double r = (v + f1 * n1[k]) + f2 * n2[k];
-        if (lev < g.L && on_ring(g, i, j)) {
-            const double hc = gridstep(g, lev);
-            const double fac = 0.25 * g.dt / (g.Re * (hc * hc));
-            r = r + apply_bc_at(0.0, gam_old + (b + 1) * bs, g, i, j, fac);
-        }
-        rhs[k] = r;
+        T *q = p + b * bs + (long long)(i - 1) + (long long)ld * (j - 1);
+        *q = (T)((double)*q - v);
     }
 };
 
@@ -126,30 +122,34 @@ struct Mult {
 // X pass: DST along x of rows (ja, jb) = (2p+1, 2p+2) of each batch field.
 // D is the line transform (Pow2Dst<M> or GenericDst); NG line pairs per block.
 template <class D, int NG, class In, class Out>
-__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) xpass_kernel(In in, Out out, Plan pl, int nrows) {
-    extern __shared__ double2 smem[];
+__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
+    xpass_kernel(In in, Out out, PlanT<typename D::Real> pl, int nrows) {
+    using T = typename D::Real;
+    using C = typename D::C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *smem = reinterpret_cast<C *>(smem_raw);
     constexpr int TPF = D::TPF;
     const int M = pl.M;
     const int G = D::smem_len(M);
     const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
-    double2 *buf = smem + g * G;
-    double2 *wt = smem + NG * G + D::NWARP * g;
+    C *buf = smem + g * G;
+    double2 *wt = reinterpret_cast<double2 *>(smem_raw + scratch_offset<D>(M, NG)) + D::NWARP * g;
     const int b = blockIdx.y;
     const int pair = blockIdx.x * NG + g;
     const int ja = 2 * pair + 1, jb = 2 * pair + 2;
     const bool va = ja <= nrows, vb = jb <= nrows;
     for (int i = t; i <= M; i += TPF) {
-        double2 z = make_double2(0.0, 0.0);
+        C z = Cx<T>::make(0, 0);
         if (i >= 1 && i < M) {
-            if (va) z.x = in(b, i, ja);
-            if (vb) z.y = in(b, i, jb);
+            if (va) z.x = (T)in(b, i, ja);
+            if (vb) z.y = (T)in(b, i, jb);
         }
         buf[D::idx(i)] = z;
     }
     __syncthreads();
     D::dst(buf, pl, t, wt);
     for (int i = 1 + t; i < M; i += TPF) {
-        const double2 y = buf[D::idx(i)];
+        const C y = buf[D::idx(i)];
         if (va) out(b, i, ja, y.x);
         if (vb) out(b, i, jb, y.y);
     }
@@ -158,26 +158,30 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) xpass_kernel(
 // Y pass: for each column i, x[i, :] = DST_y(mult(i, :) * DST_y(in[i, :])).
 // A block owns 2*NG adjacent columns; loads and stores are row-coalesced.
 template <class D, int NG>
-__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) ypass_kernel(const double *__restrict__ in, double *__restrict__ out,
-                                                           long long bs, int ncols, Plan pl, Mult mult) {
-    extern __shared__ double2 smem[];
+__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
+    ypass_kernel(const typename D::Real *__restrict__ in, typename D::Real *__restrict__ out, long long bs, int ncols,
+                 PlanT<typename D::Real> pl, Mult mult) {
+    using T = typename D::Real;
+    using C = typename D::C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *smem = reinterpret_cast<C *>(smem_raw);
     constexpr int TPF = D::TPF;
     const int M = pl.M;
     const int G = D::smem_len(M);
     const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
-    double2 *buf = smem + g * G;
-    double2 *wt = smem + NG * G + D::NWARP * g;
+    C *buf = smem + g * G;
+    double2 *wt = reinterpret_cast<double2 *>(smem_raw + scratch_offset<D>(M, NG)) + D::NWARP * g;
     const int b = blockIdx.y;
     const int c0 = blockIdx.x * 2 * NG;  // 0-based first column of the block
-    const double *src = in + b * bs;
-    double *dst = out + b * bs;
+    const T *src = in + b * bs;
+    T *dst = out + b * bs;
     constexpr int W = 2 * NG;
     for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
         const int c = e % W, jj = e / W;
         const int col = c0 + c;
-        double v = 0.0;
+        T v = 0;
         if (jj >= 1 && jj < M && col < ncols) v = src[col + (long long)ncols * (jj - 1)];
-        double *slot = reinterpret_cast<double *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
+        T *slot = reinterpret_cast<T *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
         *slot = v;
     }
     __syncthreads();
@@ -189,9 +193,9 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) ypass_kernel(
         const int ia = c0 + 2 * g + 1, ib = c0 + 2 * g + 2;  // 1-based columns
         const double cb = mult.coef(b);
         for (int jj = 1 + t; jj < M; jj += TPF) {
-            double2 y = buf[D::idx(jj)];
-            y.x *= (ia <= ncols) ? mult(cb, ia, jj) : 0.0;
-            y.y *= (ib <= ncols) ? mult(cb, ib, jj) : 0.0;
+            C y = buf[D::idx(jj)];
+            y.x = (T)(y.x * ((ia <= ncols) ? mult(cb, ia, jj) : 0.0));
+            y.y = (T)(y.y * ((ib <= ncols) ? mult(cb, ib, jj) : 0.0));
             buf[D::idx(jj)] = y;
         }
         __syncthreads();
@@ -200,7 +204,7 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) ypass_kernel(
         const int c = e % W, jj = e / W;
         const int col = c0 + c;
         if (jj >= 1 && jj < M && col < ncols) {
-            const double *slot = reinterpret_cast<const double *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
+            const T *slot = reinterpret_cast<const T *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
             dst[col + (long long)ncols * (jj - 1)] = *slot;
         }
     }
@@ -217,29 +221,33 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG)) ypass_kernel(
 // X pass: row j of level b as one complex line z = Gamma + i rest.
 template <class D, int NG>
 __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
-    xpass_trial_kernel(const double *__restrict__ gam, const double *__restrict__ rest, double *__restrict__ t1,
-                       double *__restrict__ t2, long long bs, int ld, Plan pl, int nrows) {
-    extern __shared__ double2 smem[];
+    xpass_trial_kernel(const typename D::Real *__restrict__ gam, const typename D::Real *__restrict__ rest,
+                       typename D::Real *__restrict__ t1, typename D::Real *__restrict__ t2, long long bs, int ld,
+                       PlanT<typename D::Real> pl, int nrows) {
+    using T = typename D::Real;
+    using C = typename D::C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *smem = reinterpret_cast<C *>(smem_raw);
     constexpr int TPF = D::TPF;
     const int M = pl.M;
     const int G = D::smem_len(M);
     const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
-    double2 *buf = smem + g * G;
-    double2 *wt = smem + NG * G + D::NWARP * g;
+    C *buf = smem + g * G;
+    double2 *wt = reinterpret_cast<double2 *>(smem_raw + scratch_offset<D>(M, NG)) + D::NWARP * g;
     const int b = blockIdx.y;
     const int j = blockIdx.x * NG + g + 1;
     const bool valid = j <= nrows;
     const long long row = b * bs + (long long)ld * (j - 1);
     for (int i = t; i <= M; i += TPF) {
-        double2 z = make_double2(0.0, 0.0);
-        if (valid && i >= 1 && i < M) z = make_double2(gam[row + i - 1], rest[row + i - 1]);
+        C z = Cx<T>::make(0, 0);
+        if (valid && i >= 1 && i < M) z = Cx<T>::make(gam[row + i - 1], rest[row + i - 1]);
         buf[D::idx(i)] = z;
     }
     __syncthreads();
     D::dst(buf, pl, t, wt);
     if (valid)
         for (int i = 1 + t; i < M; i += TPF) {
-            const double2 y = buf[D::idx(i)];
+            const C y = buf[D::idx(i)];
             t1[row + i - 1] = y.x;
             t2[row + i - 1] = y.y;
         }
@@ -252,26 +260,30 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
 // phase 2 transforms the real v of two columns packed as one complex line.
 template <class D, int NG>
 __global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
-    ypass_trial_kernel(const double *__restrict__ t1, const double *__restrict__ t2, double *__restrict__ out,
-                       long long bs, int ncols, Plan pl, Mult mult) {
-    extern __shared__ double2 smem[];
+    ypass_trial_kernel(const typename D::Real *__restrict__ t1, const typename D::Real *__restrict__ t2,
+                       typename D::Real *__restrict__ out, long long bs, int ncols, PlanT<typename D::Real> pl,
+                       Mult mult) {
+    using T = typename D::Real;
+    using C = typename D::C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *smem = reinterpret_cast<C *>(smem_raw);
     constexpr int TPF = D::TPF;
     constexpr int W = 2 * NG;
     const int M = pl.M;
     const int G = D::smem_len(M);
     const int g = threadIdx.x / TPF, t = threadIdx.x % TPF;
-    double2 *wt = smem + W * G + D::NWARP * g;
+    double2 *wt = reinterpret_cast<double2 *>(smem_raw + scratch_offset<D>(M, W)) + D::NWARP * g;
     const int b = blockIdx.y;
     const int c0 = blockIdx.x * W;  // 0-based first column
-    const double *s1 = t1 + b * bs, *s2 = t2 + b * bs;
-    double *dst = out + b * bs;
+    const T *s1 = t1 + b * bs, *s2 = t2 + b * bs;
+    T *dst = out + b * bs;
     for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
         const int c = e % W, jj = e / W;
         const int col = c0 + c;
-        double2 z = make_double2(0.0, 0.0);
+        C z = Cx<T>::make(0, 0);
         if (jj >= 1 && jj < M && col < ncols) {
             const long long o = col + (long long)ncols * (jj - 1);
-            z = make_double2(s1[o], s2[o]);
+            z = Cx<T>::make(s1[o], s2[o]);
         }
         smem[c * G + D::idx(jj)] = z;
     }
@@ -281,26 +293,26 @@ __global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
 #pragma unroll 1
     for (int r = 0; r < 2; ++r) {
         const int c = r * NG + g;
-        double2 *buf = smem + c * G;
+        C *buf = smem + c * G;
         D::dst(buf, pl, t, wt);
         const int col1 = c0 + c + 1;  // 1-based column
         const bool ok = col1 <= ncols;
         const double cxv = ok ? __ldg(&mult.cx[col1]) : 0.0;
         for (int jj = 1 + t; jj < M; jj += TPF) {
-            const double2 y = buf[D::idx(jj)];
+            const C y = buf[D::idx(jj)];
             double v = 0.0;
             if (ok) {
                 const double lam = -2 * ((cxv + __ldg(&mult.cy[jj])) - 2);
-                v = (y.x * (1 - lam * cb) + y.y) * (scale * recip(1 + lam * cb));
+                v = ((double)y.x * (1 - lam * cb) + (double)y.y) * (scale * recip(1 + lam * cb));
             }
-            buf[D::idx(jj)] = make_double2(v, 0.0);
+            buf[D::idx(jj)] = Cx<T>::make((T)v, 0);
         }
         __syncthreads();
     }
     // phase 2: pack columns (2g, 2g+1) into buffer 2g
     {
-        double2 *ba = smem + (2 * g) * G;
-        const double2 *bb = smem + (2 * g + 1) * G;
+        C *ba = smem + (2 * g) * G;
+        const C *bb = smem + (2 * g + 1) * G;
         for (int jj = 1 + t; jj < M; jj += TPF) ba[D::idx(jj)].y = bb[D::idx(jj)].x;
         __syncthreads();
         D::dst(ba, pl, t, wt);
@@ -309,7 +321,7 @@ __global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
         const int c = e % W, jj = e / W;
         const int col = c0 + c;
         if (jj >= 1 && jj < M && col < ncols) {
-            const double2 y = smem[(c & ~1) * G + D::idx(jj)];
+            const C y = smem[(c & ~1) * G + D::idx(jj)];
             dst[col + (long long)ncols * (jj - 1)] = (c & 1) ? y.y : y.x;
         }
     }
@@ -321,26 +333,32 @@ __global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
 
 // nonlinear (src/fluid.jl:441-455) = rot(direct_product(avg_flux(q + q0), Gamma, Gamma_bc)) / hc^2,
 // with Gamma_bc = 0.25 get_bc(Gamma[:, lev+1]) (src/fluid.jl:473-483).  Batch b = level - 1.
+template <class T>
 struct NonlinArgs {
-    const double *q;      // nq x L
-    const double *gam;    // ng x L
-    double *out;          // ng x L (state.nonlin[1])
-    const double *n2;     // ng x L (state.nonlin[2]); with rest != nullptr
-    double *rest;         // ng x L: dt (1.5 N1 - 0.5 N2) + rhsbc, or nullptr
+    const T *q;           // nq x L
+    const T *gam;         // ng x L
+    T *out;               // ng x L (state.nonlin[1])
+    const T *n2;          // ng x L (state.nonlin[2]); with rest != nullptr
+    T *rest;              // ng x L: dt (1.5 N1 - 0.5 N2) + rhsbc, or nullptr
     const StepDev *prm;
     Grid g;
 };
 
-__device__ __forceinline__ double avg_qx(const NonlinArgs &a, const double *q, int lev, int i, int j) {
+template <class T>
+__device__ __forceinline__ double avg_qx(const NonlinArgs<T> &a, const T *q, int lev, int i, int j) {
     const Grid &g = a.g;
-    return (q[UI(i, j)] + q[UI(i, j - 1)] + base_flux_x(g, a.prm, lev, i, j) + base_flux_x(g, a.prm, lev, i, j - 1)) / 2;
+    return ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + base_flux_x(g, a.prm, lev, i, j) +
+            base_flux_x(g, a.prm, lev, i, j - 1)) / 2;
 }
-__device__ __forceinline__ double avg_qy(const NonlinArgs &a, const double *q, long long nu, int lev, int i, int j) {
+template <class T>
+__device__ __forceinline__ double avg_qy(const NonlinArgs<T> &a, const T *q, long long nu, int lev, int i, int j) {
     const Grid &g = a.g;
-    return (q[VI(i, j)] + q[VI(i - 1, j)] + base_flux_y(g, a.prm, lev, i, j) + base_flux_y(g, a.prm, lev, i - 1, j)) / 2;
+    return ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + base_flux_y(g, a.prm, lev, i, j) +
+            base_flux_y(g, a.prm, lev, i - 1, j)) / 2;
 }
 
-__global__ void nonlinear_kernel(NonlinArgs a) {
+template <class T>
+__global__ void nonlinear_kernel(NonlinArgs<T> a) {
     const Grid &g = a.g;
     const int nx = g.nx, ny = g.ny;
     const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -349,41 +367,42 @@ __global__ void nonlinear_kernel(NonlinArgs a) {
     if (I > nx - 1 || J > ny - 1) return;
     const long long nq = (long long)(nx + 1) * ny + (long long)nx * (ny + 1), ng = (long long)(nx - 1) * (ny - 1);
     const long long nu = (long long)(nx + 1) * ny;
-    const double *q = a.q + b * nq;
-    const double *G = a.gam + b * ng;
-    const double *C = lev < g.L ? a.gam + (b + 1) * ng : nullptr;
+    const T *q = a.q + b * nq;
+    const T *Gt = a.gam + b * ng;
+    const T *C = lev < g.L ? a.gam + (b + 1) * ng : nullptr;
+    auto G = [&](long long k) -> double { return (double)Gt[k]; };
     // x-flux product at (i, j), i in 2..nx  (direct_product_loops!, fluid.jl:396-415)
     auto fqx = [&](int i, int j) -> double {
         if (j == 1)
-            return (avg_qy(a, q, nu, lev, i, 2) * G[GI(i - 1, 1)] +
+            return (avg_qy(a, q, nu, lev, i, 2) * G(GI(i - 1, 1)) +
                     avg_qy(a, q, nu, lev, i, 1) * (getbc(C, g, SIDE_B, i) * 0.25)) / 2;
         if (j == ny)
-            return (avg_qy(a, q, nu, lev, i, ny) * G[GI(i - 1, ny - 1)] +
+            return (avg_qy(a, q, nu, lev, i, ny) * G(GI(i - 1, ny - 1)) +
                     avg_qy(a, q, nu, lev, i, ny + 1) * (getbc(C, g, SIDE_T, i) * 0.25)) / 2;
-        return (avg_qy(a, q, nu, lev, i, j + 1) * G[GI(i - 1, j)] + avg_qy(a, q, nu, lev, i, j) * G[GI(i - 1, j - 1)]) / 2;
+        return (avg_qy(a, q, nu, lev, i, j + 1) * G(GI(i - 1, j)) + avg_qy(a, q, nu, lev, i, j) * G(GI(i - 1, j - 1))) / 2;
     };
     // y-flux product at (i, j), j in 2..ny  (fluid.jl:417-436)
     auto fqy = [&](int i, int j) -> double {
         if (i == 1)
-            return -(avg_qx(a, q, lev, 2, j) * G[GI(1, j - 1)] + avg_qx(a, q, lev, 1, j) * (getbc(C, g, SIDE_L, j) * 0.25)) / 2;
+            return -(avg_qx(a, q, lev, 2, j) * G(GI(1, j - 1)) + avg_qx(a, q, lev, 1, j) * (getbc(C, g, SIDE_L, j) * 0.25)) / 2;
         if (i == nx)
-            return -(avg_qx(a, q, lev, nx, j) * G[GI(nx - 1, j - 1)] +
+            return -(avg_qx(a, q, lev, nx, j) * G(GI(nx - 1, j - 1)) +
                      avg_qx(a, q, lev, nx + 1, j) * (getbc(C, g, SIDE_R, j) * 0.25)) / 2;
-        return -(avg_qx(a, q, lev, i + 1, j) * G[GI(i, j - 1)] + avg_qx(a, q, lev, i, j) * G[GI(i - 1, j - 1)]) / 2;
+        return -(avg_qx(a, q, lev, i + 1, j) * G(GI(i, j - 1)) + avg_qx(a, q, lev, i, j) * G(GI(i - 1, j - 1))) / 2;
     };
     // rot! at Gamma(I, J) with i = I+1, j = J+1 (fluid.jl:106-108)
     const double r = (fqx(I + 1, J) - fqx(I + 1, J + 1)) + (fqy(I + 1, J + 1) - fqy(I, J + 1));
     const double hc = gridstep(g, lev);
     const double n1 = r * (1 / (hc * hc));
-    a.out[b * ng + GI(I, J)] = n1;
+    a.out[b * ng + GI(I, J)] = (T)n1;
     if (a.rest) {
         // rest = dt b1 N1 + dt b2 N2 + rhsbc (fluid.jl:487-493), rhsbc = apply_bc!(0, get_bc(..); fac)
-        double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * a.n2[b * ng + GI(I, J)];
+        double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * (double)a.n2[b * ng + GI(I, J)];
         if (lev < g.L && on_ring(g, I, J)) {
             const double fac = 0.25 * g.dt / (g.Re * (hc * hc));
             v = v + apply_bc_at(0.0, C, g, I, J, fac);
         }
-        a.rest[b * ng + GI(I, J)] = v;
+        a.rest[b * ng + GI(I, J)] = (T)v;
     }
 }
 
@@ -391,8 +410,9 @@ __global__ void nonlinear_kernel(NonlinArgs a) {
 // A 2D grid over the faces: blockIdx.y < ceil((ny+1)/by) covers the x faces
 // (rows j <= ny) and, offset by that count, the y faces (rows j <= ny+1).
 // Batch b (blockIdx.z) uses psi + b*bs, q + b*qbs, coarse + b*cbs.
-__global__ void curl_kernel(double *__restrict__ qout, long long qbs, const double *__restrict__ psi, long long bs,
-                            const double *__restrict__ coarse, long long cbs, Grid g) {
+template <class T>
+__global__ void curl_kernel(T *__restrict__ qout, long long qbs, const T *__restrict__ psi, long long bs,
+                            const T *__restrict__ coarse, long long cbs, Grid g) {
     const int nx = g.nx, ny = g.ny;
     const long long nu = (long long)(nx + 1) * ny;
     const int rows_u = (ny + blockDim.y - 1) / blockDim.y;
@@ -400,9 +420,10 @@ __global__ void curl_kernel(double *__restrict__ qout, long long qbs, const doub
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = (yface ? blockIdx.y - rows_u : blockIdx.y) * blockDim.y + threadIdx.y + 1;
     const int b = blockIdx.z;
-    const double *P = psi + b * bs;
-    const double *C = coarse ? coarse + b * cbs : nullptr;
-    double *q = qout + b * qbs;
+    const T *Pt = psi + b * bs;
+    const T *C = coarse ? coarse + b * cbs : nullptr;
+    T *q = qout + b * qbs;
+    auto P = [&](long long k) -> double { return (double)Pt[k]; };
     if (!yface) {
         if (i > nx + 1 || j > ny) return;
         double v;
@@ -411,12 +432,12 @@ __global__ void curl_kernel(double *__restrict__ qout, long long qbs, const doub
         else if (i == nx + 1)
             v = getbc(C, g, SIDE_R, j + 1) - getbc(C, g, SIDE_R, j);
         else if (j == 1)
-            v = P[GI(i - 1, 1)] - getbc(C, g, SIDE_B, i);
+            v = P(GI(i - 1, 1)) - getbc(C, g, SIDE_B, i);
         else if (j == ny)
-            v = getbc(C, g, SIDE_T, i) - P[GI(i - 1, ny - 1)];
+            v = getbc(C, g, SIDE_T, i) - P(GI(i - 1, ny - 1));
         else
-            v = P[GI(i - 1, j)] - P[GI(i - 1, j - 1)];
-        q[UI(i, j)] = v;
+            v = P(GI(i - 1, j)) - P(GI(i - 1, j - 1));
+        q[UI(i, j)] = (T)v;
     } else {
         if (i > nx || j > ny + 1) return;
         double v;
@@ -425,29 +446,31 @@ __global__ void curl_kernel(double *__restrict__ qout, long long qbs, const doub
         else if (j == ny + 1)
             v = getbc(C, g, SIDE_T, i) - getbc(C, g, SIDE_T, i + 1);
         else if (i == 1)
-            v = getbc(C, g, SIDE_L, j) - P[GI(1, j - 1)];
+            v = getbc(C, g, SIDE_L, j) - P(GI(1, j - 1));
         else if (i == nx)
-            v = P[GI(nx - 1, j - 1)] - getbc(C, g, SIDE_R, j);
+            v = P(GI(nx - 1, j - 1)) - getbc(C, g, SIDE_R, j);
         else
-            v = P[GI(i - 1, j - 1)] - P[GI(i, j - 1)];
-        q[VI(i, j)] = v;
+            v = P(GI(i - 1, j - 1)) - P(GI(i, j - 1));
+        q[VI(i, j)] = (T)v;
     }
 }
 
 // coarsify! (src/fluid.jl:208-228): fine level -> central block of the next coarser level.
-__global__ void coarsify_kernel(double *__restrict__ coarse, const double *__restrict__ fine, long long bs, Grid g) {
+template <class T>
+__global__ void coarsify_kernel(T *__restrict__ coarse, const T *__restrict__ fine, long long bs, Grid g) {
     const int nx = g.nx, ny = g.ny;
     const int ni = (nx / 2 - 2 - (-nx / 2 + 2)) / 2 + 1, nic = (nx / 4 - 1) - (-nx / 4 + 1) + 1;
     const int nj = (ny / 2 - 2 - (-ny / 2 + 2)) / 2 + 1, njc = (ny / 4 - 1) - (-ny / 4 + 1) + 1;
     const int ci = ni < nic ? ni : nic, cj = nj < njc ? nj : njc;
     const int a = blockIdx.x * blockDim.x + threadIdx.x, bb = blockIdx.y * blockDim.y + threadIdx.y;
     if (a >= ci || bb >= cj) return;
-    const double *G = fine + blockIdx.z * bs;
-    double *Gc = coarse + blockIdx.z * bs;
+    const T *Gf = fine + blockIdx.z * bs;
+    T *Gc = coarse + blockIdx.z * bs;
+    auto G = [&](long long k) -> double { return (double)Gf[k]; };
     const int i = nx / 2 + (-nx / 2 + 2) + 2 * a, ic = nx / 2 + (-nx / 4 + 1) + a;
     const int j = ny / 2 + (-ny / 2 + 2) + 2 * bb, jc = ny / 2 + (-ny / 4 + 1) + bb;
-    Gc[GI(ic, jc)] = G[GI(i, j)] + 0.5 * (G[GI(i + 1, j)] + G[GI(i, j + 1)] + G[GI(i - 1, j)] + G[GI(i, j - 1)]) +
-                     0.25 * (G[GI(i + 1, j + 1)] + G[GI(i + 1, j - 1)] + G[GI(i - 1, j - 1)] + G[GI(i - 1, j + 1)]);
+    Gc[GI(ic, jc)] = (T)(G(GI(i, j)) + 0.5 * (G(GI(i + 1, j)) + G(GI(i, j + 1)) + G(GI(i - 1, j)) + G(GI(i, j - 1))) +
+                         0.25 * (G(GI(i + 1, j + 1)) + G(GI(i + 1, j - 1)) + G(GI(i - 1, j - 1)) + G(GI(i - 1, j + 1))));
 }
 
 // x = Binv z for the precomputed B^-1 (src/coupling.jl:187-192), column-major n x n.

@@ -39,9 +39,13 @@ def _init_static_panels(state: State):
 
 
 class GpuCnabSolver(AbstractSolver):
-    """CnabSolver(state; cg=(maxiter, reltol, abstol)) on the GPU (FP64)."""
+    """CnabSolver(state; cg=(maxiter, reltol, abstol)) on the GPU.
 
-    def __init__(self, state: State, *, cg: Optional[dict] = None, device: int = 0):
+    precision="fp64" is the plain drop-in path; precision="fp32" is the mixed
+    precision path (FP32 fields and transforms; FP64 scans, boundary values,
+    CG, force sums and B^-1)."""
+
+    def __init__(self, state: State, *, cg: Optional[dict] = None, device: int = 0, precision: str = "fp64"):
         self.lib = _abi.load()
         self.state = state
         prob = state.prob
@@ -61,6 +65,8 @@ class GpuCnabSolver(AbstractSolver):
         opt = _abi.ibpm_options()
         self.lib.ibpm_default_options(C.byref(opt))
         opt.device = device
+        opt.precision = {"fp64": _abi.IBPM_FP64, "fp32": _abi.IBPM_FP32}[precision]
+        self.precision = precision
         for k, v in (cg or {}).items():
             setattr(opt, {"maxiter": "cg_maxiter", "reltol": "cg_reltol", "abstol": "cg_abstol"}[k], v)
         rc = self.lib.ibpm_create(C.byref(p), C.byref(opt), C.byref(self._h))

@@ -1,0 +1,51 @@
+"""The mixed-precision path (FP32 fields and transforms, FP64 scans, boundary
+values, CG, force sums and B^-1) against the FP64 path: vorticity relative L2
+<= 1e-5 and |ΔC_D|, |ΔC_L| <= 1e-4, the chosen form's accuracy bar."""
+import numpy as np
+import pytest
+
+from fixtures import rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL_VORT = 1e-5
+TOL_COEF = 1e-4
+
+
+def _coeffs(fb_total, U=1.0, Lref=1.0):
+    return 2 * np.asarray(fb_total) / (U * U * Lref)
+
+
+@pytest.mark.parametrize("builder,nsteps", [("cylinder_re100_200", 40), ("small_plate_256", 40)])
+def test_fp32_matches_fp64(ib, builder, nsteps):
+    if builder == "small_plate_256":
+        prob = ib.configs.plate(4.0 / 256, (-1.0, 3.0), (-2.0, 2.0), 4, 65, 200.0, 0.004, 30.0)
+    else:
+        prob = getattr(ib.configs, builder)()
+    s64 = ib.State(prob)
+    s32 = ib.State(prob)
+    g64 = ib.create_solver(s64, precision="fp64")
+    g32 = ib.create_solver(s32, precision="fp32")
+    worst = 0.0
+    for _ in range(nsteps):
+        g64.advance_()
+        g32.advance_()
+        d = np.abs(_coeffs(g64.total_force()) - _coeffs(g32.total_force())).max()
+        worst = max(worst, d)
+    g64.getstate()
+    g32.getstate()
+    assert worst <= TOL_COEF, worst
+    assert rel_l2(s32.Gamma, s64.Gamma) <= TOL_VORT
+
+
+def test_fp32_moving_body_cg(ib):
+    import glob, os
+    from fixtures import problem_from_fixture
+    fx = np.load(os.path.join(os.path.dirname(__file__), "golden", "plate32_moving.npz"))
+    _, s64 = problem_from_fixture(ib, fx)
+    _, s32 = problem_from_fixture(ib, fx)
+    g64 = ib.create_solver(s64, precision="fp64")
+    g32 = ib.create_solver(s32, precision="fp32")
+    for _ in range(int(fx["nsteps"])):
+        g64.advance_()
+        g32.advance_()
+    assert np.abs(g64.total_force() - g32.total_force()).max() <= TOL_COEF * max(1, np.abs(g64.total_force()).max())
