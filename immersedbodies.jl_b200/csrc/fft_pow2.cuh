@@ -160,23 +160,23 @@ struct DftC<16, C> {
 // Every stage has NB = M/R butterflies with NB % 16 == 0 and a stride NS that
 // is 1 or a multiple of 16, so all padded shared-memory offsets of a stage are
 // compile-time constants added to one per-thread base.
+// A plan lists the radices R0..R4 (1 = unused); TPF threads per line pair;
+// OCC the resident threads per SM the kernels are compiled for (it caps the
+// registers per thread at 65536 / OCC).
+template <int TPF_, int R0_, int R1_, int R2_, int R3_ = 1, int R4_ = 1, int OCC_ = 512>
+struct PlanCT {
+    static constexpr int TPF = TPF_;
+    static constexpr int OCC = OCC_;
+    static constexpr int R0 = R0_, R1 = R1_, R2 = R2_, R3 = R3_, R4 = R4_;
+};
 template <int M>
 struct Pow2Plan;
 template <>
-struct Pow2Plan<1024> {
-    static constexpr int TPF = 64;
-    static constexpr int R0 = 16, R1 = 16, R2 = 4;
-};
+struct Pow2Plan<1024> : PlanCT<64, 16, 16, 4> {};
 template <>
-struct Pow2Plan<512> {
-    static constexpr int TPF = 64;
-    static constexpr int R0 = 16, R1 = 8, R2 = 4;
-};
+struct Pow2Plan<512> : PlanCT<64, 16, 8, 4> {};
 template <>
-struct Pow2Plan<256> {
-    static constexpr int TPF = 32;
-    static constexpr int R0 = 16, R1 = 4, R2 = 4;
-};
+struct Pow2Plan<256> : PlanCT<32, 16, 4, 4> {};
 
 // padded offset of (base + c) given that base % 16 == b16 is known to leave room
 template <int NS, int R, int r>
@@ -186,6 +186,15 @@ struct WriteOff {
     static constexpr int value = NS == 1 ? r : r * NS * 17 / 16;
 };
 
+// Padded offset of the r-th output of a butterfly relative to its first output
+// d = (j / NS) NS R + (j % NS): a constant when NS is a multiple of 16 (then
+// d + r NS crosses r NS / 16 pads) or when NS R divides 16 (then the R outputs
+// stay inside one 16-entry row).
+template <int R, int NS>
+__host__ __device__ constexpr int write_off(int r) {
+    return NS % 16 == 0 ? r * NS * 17 / 16 : r * NS;
+}
+
 // One Stockham stage with compile-time sizes on a padded buffer.
 template <int M, int R, int NS, int TPF, class C>
 __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t) {
@@ -194,8 +203,7 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t
     constexpr bool ALL = NB >= TPF;              // every thread has a butterfly
     constexpr int TWS = M / (NS * R);
     static_assert((NB % TPF == 0 || TPF % NB == 0) && NB % 16 == 0, "stage layout");
-    static_assert(NS == 1 || NS % 16 == 0, "stage stride");
-    static_assert(NS != 1 || 16 % R == 0, "first-stage radix");
+    static_assert(NS % 16 == 0 || 16 % (NS * R) == 0, "stage stride");
     constexpr int RSTEP = NB * 17 / 16;  // padded distance between the R inputs
     C v[K][R];
 #pragma unroll
@@ -225,14 +233,16 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t
         const int k = j % NS;
         C *dst = buf + pad16((j / NS) * NS * R + k);
 #pragma unroll
-        for (int r = 0; r < R; ++r) dst[NS == 1 ? r : r * NS * 17 / 16] = v[kb][r];
+        for (int r = 0; r < R; ++r) dst[write_off<R, NS>(r)] = v[kb][r];
     }
     __syncthreads();
 }
 
-template <int M, class T>
+template <int M, class T, class PL = Pow2Plan<M>>
 struct Pow2Dst {
-    using P = Pow2Plan<M>;
+    using P = PL;
+    static constexpr int OCC = P::OCC;
+    static constexpr int MC = M;  // compile-time transform length
     using Real = T;
     using C = typename Cx<T>::type;
     static constexpr int TPF = P::TPF;
@@ -242,27 +252,38 @@ struct Pow2Dst {
     static __device__ __forceinline__ int idx(int i) { return pad16(i); }
 
     static __device__ __forceinline__ void fft(C *buf, const C *__restrict__ tw, int t) {
+        constexpr int N1 = P::R0, N2 = N1 * P::R1, N3 = N2 * P::R2, N4 = N3 * P::R3;
+        static_assert(N4 * P::R4 == M, "plan must factor M");
         stage_ct<M, P::R0, 1, TPF, C>(buf, tw, t);
-        stage_ct<M, P::R1, P::R0, TPF, C>(buf, tw, t);
-        stage_ct<M, P::R2, P::R0 * P::R1, TPF, C>(buf, tw, t);
-        static_assert(P::R0 * P::R1 * P::R2 == M, "plan must factor M");
+        stage_ct<M, P::R1, N1, TPF, C>(buf, tw, t);
+        stage_ct<M, P::R2, N2, TPF, C>(buf, tw, t);
+        if constexpr (P::R3 > 1) stage_ct<M, P::R3, N3, TPF, C>(buf, tw, t);
+        if constexpr (P::R4 > 1) stage_ct<M, P::R4, N4, TPF, C>(buf, tw, t);
     }
 
     // pre-twiddle in place; buf[1..M-1] hold z, buf[0], buf[M] are read as 0
     static __device__ __forceinline__ void pre(C *buf, const T *__restrict__ sn, int t) {
         constexpr int H = M / 2;
+        constexpr int NIT = (H + 1 + TPF - 1) / TPF;
+        T s[NIT];
 #pragma unroll
-        for (int j = t; j <= H; j += TPF) {
+        for (int k = 0; k < NIT; ++k) {  // issue the table loads first
+            const int j = t + k * TPF;
+            s[k] = j <= H ? __ldg(&sn[j]) : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NIT; ++k) {
+            const int j = t + k * TPF;
+            if (j > H) break;
             if (j == 0) {
                 buf[0] = Cx<T>::make(0, 0);
             } else if (j == H) {
                 const C z = buf[pad16(H)];
-                buf[pad16(H)] = __ldg(&sn[H]) * (z + z);
+                buf[pad16(H)] = s[k] * (z + z);
             } else {
-                const T s = __ldg(&sn[j]);
                 const C a = buf[pad16(j)], b = buf[pad16(M - j)];
-                buf[pad16(j)] = s * (a + b) + (T)0.5 * (a - b);
-                buf[pad16(M - j)] = s * (a + b) + (T)0.5 * (b - a);
+                buf[pad16(j)] = s[k] * (a + b) + (T)0.5 * (a - b);
+                buf[pad16(M - j)] = s[k] * (a + b) + (T)0.5 * (b - a);
             }
         }
         __syncthreads();
@@ -336,6 +357,8 @@ struct Pow2Dst {
 // of the form 2^a 3^b 5^c), unpadded.
 template <class T>
 struct GenericDst {
+    static constexpr int OCC = 512;
+    static constexpr int MC = 0;  // transform length known only at run time
     using Real = T;
     using C = typename Cx<T>::type;
     static constexpr int TPF = kTPF;

@@ -238,41 +238,59 @@ struct Engine final : ibpm_handle {
     // Dispatch on the transform length: compile-time power-of-two transforms
     // for M in {128, 256, 512, 1024}, the runtime mixed-radix one otherwise.
     template <class D, class In, class Out>
-    void xpass_t(In in, Out out, int nbatch) {
+    void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch) {
         const int pairs = (ny - 1 + 1) / 2;
         const dim3 grid((pairs + kNG - 1) / kNG, nbatch);
-        const size_t sm = pass_smem<D>(plx.M, kNG, kNG);
-        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, plx, ny - 1);
+        const size_t sm = pass_smem<D>(pl.M, kNG, kNG);
+        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, pl, ny - 1);
     }
-    template <class In, class Out>
+    // X pass with transforms of element type R (the engine's T, or double for
+    // the FP32 engine's FP64 level-1 solve); In/Out convert at the boundary.
+    template <class R = T, class In, class Out>
     void xpass(In in, Out out, int nbatch) {
+        const PlanT<R> &pl = plan_x<R>();
         const int pe = prof_begin();
-        switch (plx.M) {
-            case 1024: xpass_t<Pow2Dst<1024, T>>(in, out, nbatch); break;
-            case 512: xpass_t<Pow2Dst<512, T>>(in, out, nbatch); break;
-            case 256: xpass_t<Pow2Dst<256, T>>(in, out, nbatch); break;
-            default: xpass_t<GenericDst<T>>(in, out, nbatch); break;
+        switch (pl.M) {
+            case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch); break;
+            case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch); break;
+            case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch); break;
+            default: xpass_t<GenericDst<R>>(pl, in, out, nbatch); break;
         }
         check_launch();
-        prof_end(pe, IBPM_KCLASS_XPASS, 16.0 * (double)ng * nbatch);
+        prof_end(pe, IBPM_KCLASS_XPASS, 2.0 * sizeof(R) * (double)ng * nbatch);
     }
     template <class D>
-    void ypass_t(const T *in, T *out, long long bs, int nbatch, Mult m) {
+    void ypass_t(const PlanT<typename D::Real> &pl, const typename D::Real *in, typename D::Real *out, long long bs,
+                 int nbatch, Mult m) {
         const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nbatch);
-        const size_t sm = pass_smem<D>(ply.M, kNG, kNG);
-        ypass_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(in, out, bs, nx - 1, ply, m);
+        const size_t sm = pass_smem<D>(pl.M, kNG, kNG);
+        ypass_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(in, out, bs, nx - 1, pl, m);
     }
-    void ypass(const T *in, T *out, long long bs, int nbatch, Mult m) {
+    template <class R = T>
+    void ypass(const R *in, R *out, long long bs, int nbatch, Mult m) {
+        const PlanT<R> &pl = plan_y<R>();
         const int pe = prof_begin();
-        switch (ply.M) {
-            case 1024: ypass_t<Pow2Dst<1024, T>>(in, out, bs, nbatch, m); break;
-            case 512: ypass_t<Pow2Dst<512, T>>(in, out, bs, nbatch, m); break;
-            case 256: ypass_t<Pow2Dst<256, T>>(in, out, bs, nbatch, m); break;
-            default: ypass_t<GenericDst<T>>(in, out, bs, nbatch, m); break;
+        switch (pl.M) {
+            case 1024: ypass_t<Pow2Dst<1024, R>>(pl, in, out, bs, nbatch, m); break;
+            case 512: ypass_t<Pow2Dst<512, R>>(pl, in, out, bs, nbatch, m); break;
+            case 256: ypass_t<Pow2Dst<256, R>>(pl, in, out, bs, nbatch, m); break;
+            default: ypass_t<GenericDst<R>>(pl, in, out, bs, nbatch, m); break;
         }
         check_launch();
-        prof_end(pe, IBPM_KCLASS_YPASS, 16.0 * (double)ng * nbatch);
+        prof_end(pe, IBPM_KCLASS_YPASS, 2.0 * sizeof(R) * (double)ng * nbatch);
     }
+    // transform tables of element type R: the engine's own, or FP64 ones kept by
+    // the FP32 engine for its level-1 solve
+    PlanT<double> plx_d{}, ply_d{};
+    template <class R>
+    const PlanT<R> &plan_x() const {
+        if constexpr (std::is_same<R, T>::value) return plx; else return plx_d;
+    }
+    template <class R>
+    const PlanT<R> &plan_y() const {
+        if constexpr (std::is_same<R, T>::value) return ply; else return ply_d;
+    }
+    double *psi1_hi = nullptr, *qs1_hi = nullptr, *t1_hi = nullptr, *t2_hi = nullptr;
     // Merged trial solve over all L levels: Gamma_new = Ainv(A Gamma + rest)
     template <class D>
     void trial_t(const T *Gold, const T *rest_, T *Gnew) {
@@ -333,7 +351,8 @@ struct Engine final : ibpm_handle {
     // G, psi: level 1 of batch 0, level stride ng, batch stride bs.
     // qout: level 1 of batch 0 (level stride nq, batch stride qbs); curl_all=false
     // computes q only at level 1 (the only level a caller reads).
-    void vort2flux(T *psi_, T *qout, T *Gm, long long bs, long long qbs, int nbatch, bool curl_all) {
+    void vort2flux(T *psi_, T *qout, T *Gm, long long bs, long long qbs, int nbatch, bool curl_all,
+                   bool hi1 = false) {
         for (int lev = 2; lev <= L; ++lev) {
             const int nx2 = nx / 2, ny2 = ny / 2;
             const dim3 blk(16, 16), grd((nx2 + 15) / 16, (ny2 + 15) / 16, nbatch);
@@ -343,6 +362,21 @@ struct Engine final : ibpm_handle {
         for (int lev = L; lev >= 1; --lev) {
             T *Gl = Gm + (lev - 1) * ng;
             T *Pl = psi_ + (lev - 1) * ng;
+            if (lev == 1 && hi1) {
+                // level 1 in FP64 from the FP32 coarser levels: psi1_hi and qs1_hi (x E)
+                const T *coarse = L > 1 ? psi_ + ng : nullptr;
+                if (coarse)
+                    xpass<double>(InBC<T>{Gl, coarse, bs, bs, g}, OutPlain<double>{t1_hi, ng, nx - 1}, 1);
+                else
+                    xpass<double>(in_plain(Gl, bs), OutPlain<double>{t1_hi, ng, nx - 1}, 1);
+                ypass<double>(t1_hi, t2_hi, ng, 1, mult(MULT_LAPINV, 1, 0));
+                xpass<double>(InPlain<double>{t2_hi, ng, nx - 1}, OutPlain<double>{psi1_hi, ng, nx - 1}, 1);
+                const dim3 blk(64, 4);
+                const dim3 grd((nx + 1 + 63) / 64, (ny + 3) / 4 + (ny + 1 + 3) / 4, 1);
+                curl_kernel<double, double, T><<<grd, blk, 0, st>>>(qs1_hi, 0, psi1_hi, 0, coarse, 0, g);
+                check_launch();
+                continue;
+            }
             if (lev == L)
                 xpass(in_plain(Gl, bs), out_plain(t1, ng), nbatch);
             else
@@ -353,8 +387,8 @@ struct Engine final : ibpm_handle {
                 const dim3 blk(64, 4);
                 const dim3 grd((nx + 1 + 63) / 64, (ny + 3) / 4 + (ny + 1 + 3) / 4, nbatch);
                 const int pe = prof_begin();
-                curl_kernel<<<grd, blk, 0, st>>>(qout + (lev - 1) * nq, qbs, Pl, bs, lev < L ? psi_ + lev * ng : nullptr,
-                                                 bs, g);
+                curl_kernel<T, T, T><<<grd, blk, 0, st>>>(qout + (lev - 1) * nq, qbs, Pl, bs,
+                                                          lev < L ? psi_ + lev * ng : nullptr, bs, g);
                 check_launch();
                 prof_end(pe, IBPM_KCLASS_CURL, 8.0 * (double)(ng + nq) * nbatch);
             }
@@ -423,6 +457,7 @@ struct Engine final : ibpm_handle {
     void download(double *dst, const T *src, size_t n);
 
     void init(const ibpm_problem *p, const ibpm_options &o);
+    bool hi_level1 = false;
     ibpm_problem problem_copy{};
     T *diag_q = nullptr;
     void set_state(const ibpm_state_view *s) override;
@@ -489,6 +524,34 @@ void Engine<T>::setup() {
     };
     tables(nx, twx, snx, cx, plx);
     tables(ny, twy, sny, cy, ply);
+    if (!std::is_same<T, double>::value) {
+        hi_level1 = true;
+        if (const char *e = getenv("IBPM_FP32_LEVEL1")) hi_level1 = e[0] != '0';
+        if (!make_plan(nx, plx_d) || !make_plan(ny, ply_d)) throw ApiError{IBPM_ERR_INVALID, "bad transform size"};
+        auto dtables = [&](int M, PlanT<double> &pl) {
+            std::vector<double2> htw(M);
+            std::vector<double> hsn(M + 1);
+            for (int k = 0; k < M; ++k) {
+                const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)M;
+                htw[k] = make_double2((double)cosl(a), (double)sinl(a));
+            }
+            for (int j = 0; j <= M; ++j)
+                hsn[j] = (double)sinl(3.14159265358979323846264338327950288L * (long double)j / (long double)M);
+            double2 *tw = dalloc<double2>(M);
+            double *sn = dalloc<double>(M + 1);
+            CK(cudaMemcpyAsync(tw, htw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(sn, hsn.data(), sizeof(double) * (M + 1), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+            pl.tw = tw;
+            pl.sn = sn;
+        };
+        dtables(nx, plx_d);
+        dtables(ny, ply_d);
+        psi1_hi = dalloc<double>(ng);
+        qs1_hi = dalloc<double>(nq);
+        t1_hi = dalloc<double>(ng);
+        t2_hi = dalloc<double>(ng);
+    }
 
     q = dalloc<T>(nq * L);
     psi = dalloc<T>(ng * L);
@@ -864,12 +927,17 @@ void Engine<T>::step_body() {
     }
     trial(Gold, rest, Gnew);
     nc = 1 - nc;  // _cycle!(state.nonlin)
-    vort2flux(psi, qs1, Gnew, 0, 0, 1, false);
-    // couple_surface_rigid (src/coupling.jl:236-250)
-    {
+    // couple_surface_rigid (src/coupling.jl:236-250).  The FP32 engine computes the
+    // level-1 trial flux that E interpolates in FP64: B^-1 amplifies white noise in
+    // E qs by its condition number (1e4..1e5), FP32 rounding would reach the forces.
+    if (hi_level1) {
+        vort2flux(psi, qs1, Gnew, 0, 0, 1, false, true);
+        launch_regT(P, qs1_hi, 0, Ftmp, 0, 1, 1, prm, g, st);
+    } else {
+        vort2flux(psi, qs1, Gnew, 0, 0, 1, false);
         launch_regT(P, qs1, 0, Ftmp, 0, 1, 1, prm, g, st);
-        check_launch();
     }
+    check_launch();
     const int n = 2 * np;
     if (static_bodies) {
         const int nchunk = (n + 63) / 64;

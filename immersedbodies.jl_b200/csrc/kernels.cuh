@@ -111,18 +111,21 @@ struct Mult {
         const double hc = ldexp(h, lev - 1);
         return dt / (2 * Re * (hc * hc));
     }
-    __device__ __forceinline__ double operator()(double c, int i, int j) const {
-        const double lam = -2 * ((__ldg(&cx[i]) + __ldg(&cy[j])) - 2);
+    __device__ __forceinline__ double eval(double c, double cxi, double cyj) const {
+        const double lam = -2 * ((cxi + cyj) - 2);
         if (mode == MULT_LAPINV) return scale * recip(lam);
         if (mode == MULT_AEXPL) return scale * (1 - lam * c);  // scale / (1 / (1 - lam c))
         return scale * recip(1 + lam * c);
+    }
+    __device__ __forceinline__ double operator()(double c, int i, int j) const {
+        return eval(c, __ldg(&cx[i]), __ldg(&cy[j]));
     }
 };
 
 // X pass: DST along x of rows (ja, jb) = (2p+1, 2p+2) of each batch field.
 // D is the line transform (Pow2Dst<M> or GenericDst); NG line pairs per block.
 template <class D, int NG, class In, class Out>
-__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
+__global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
     xpass_kernel(In in, Out out, PlanT<typename D::Real> pl, int nrows) {
     using T = typename D::Real;
     using C = typename D::C;
@@ -138,13 +141,32 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
     const int pair = blockIdx.x * NG + g;
     const int ja = 2 * pair + 1, jb = 2 * pair + 2;
     const bool va = ja <= nrows, vb = jb <= nrows;
-    for (int i = t; i <= M; i += TPF) {
-        C z = Cx<T>::make(0, 0);
-        if (i >= 1 && i < M) {
-            if (va) z.x = (T)in(b, i, ja);
-            if (vb) z.y = (T)in(b, i, jb);
+    if constexpr (D::MC > 0) {
+        // compile-time trip count: every global load of the thread is in flight
+        // before the first shared-memory store
+        constexpr int NIT = (D::MC + 1 + TPF - 1) / TPF;
+        T za[NIT], zb[NIT];
+#pragma unroll
+        for (int k = 0; k < NIT; ++k) {
+            const int i = t + k * TPF;
+            const bool in_line = i >= 1 && i < D::MC;
+            za[k] = (in_line && va) ? (T)in(b, i, ja) : (T)0;
+            zb[k] = (in_line && vb) ? (T)in(b, i, jb) : (T)0;
         }
-        buf[D::idx(i)] = z;
+#pragma unroll
+        for (int k = 0; k < NIT; ++k) {
+            const int i = t + k * TPF;
+            if (i <= D::MC) buf[D::idx(i)] = Cx<T>::make(za[k], zb[k]);
+        }
+    } else {
+        for (int i = t; i <= M; i += TPF) {
+            C z = Cx<T>::make(0, 0);
+            if (i >= 1 && i < M) {
+                if (va) z.x = (T)in(b, i, ja);
+                if (vb) z.y = (T)in(b, i, jb);
+            }
+            buf[D::idx(i)] = z;
+        }
     }
     __syncthreads();
     D::dst(buf, pl, t, wt);
@@ -158,7 +180,7 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
 // Y pass: for each column i, x[i, :] = DST_y(mult(i, :) * DST_y(in[i, :])).
 // A block owns 2*NG adjacent columns; loads and stores are row-coalesced.
 template <class D, int NG>
-__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
+__global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
     ypass_kernel(const typename D::Real *__restrict__ in, typename D::Real *__restrict__ out, long long bs, int ncols,
                  PlanT<typename D::Real> pl, Mult mult) {
     using T = typename D::Real;
@@ -176,13 +198,38 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
     const T *src = in + b * bs;
     T *dst = out + b * bs;
     constexpr int W = 2 * NG;
-    for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
-        const int c = e % W, jj = e / W;
-        const int col = c0 + c;
-        T v = 0;
-        if (jj >= 1 && jj < M && col < ncols) v = src[col + (long long)ncols * (jj - 1)];
-        T *slot = reinterpret_cast<T *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
-        *slot = v;
+    if constexpr (D::MC > 0) {
+        // compile-time trip count, loads issued in chunks of CH before their stores
+        constexpr int NT = NG * TPF;
+        constexpr int NIT = (W * (D::MC + 1) + NT - 1) / NT;
+        constexpr int CH = 12;
+#pragma unroll
+        for (int k0 = 0; k0 < NIT; k0 += CH) {
+            T v[CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = threadIdx.x + (k0 + k) * NT;
+                const int c = e % W, jj = e / W;
+                const int col = c0 + c;
+                v[k] = (k0 + k < NIT && jj >= 1 && jj < D::MC && col < ncols) ? src[col + (long long)ncols * (jj - 1)]
+                                                                               : (T)0;
+            }
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = threadIdx.x + (k0 + k) * NT;
+                const int c = e % W, jj = e / W;
+                if (k0 + k < NIT && jj <= D::MC) *(reinterpret_cast<T *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1)) = v[k];
+            }
+        }
+    } else {
+        for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
+            const int c = e % W, jj = e / W;
+            const int col = c0 + c;
+            T v = 0;
+            if (jj >= 1 && jj < M && col < ncols) v = src[col + (long long)ncols * (jj - 1)];
+            T *slot = reinterpret_cast<T *>(smem + (c >> 1) * G + D::idx(jj)) + (c & 1);
+            *slot = v;
+        }
     }
     __syncthreads();
     // DST, spectral multiply, DST; one loop body so the transform is emitted once
@@ -192,11 +239,31 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
         if (pass == 1) break;
         const int ia = c0 + 2 * g + 1, ib = c0 + 2 * g + 2;  // 1-based columns
         const double cb = mult.coef(b);
-        for (int jj = 1 + t; jj < M; jj += TPF) {
-            C y = buf[D::idx(jj)];
-            y.x = (T)(y.x * ((ia <= ncols) ? mult(cb, ia, jj) : 0.0));
-            y.y = (T)(y.y * ((ib <= ncols) ? mult(cb, ib, jj) : 0.0));
-            buf[D::idx(jj)] = y;
+        if constexpr (D::MC > 0) {
+            constexpr int NIT = (D::MC - 1 + TPF - 1) / TPF;
+            const double cxa = ia <= ncols ? __ldg(&mult.cx[ia]) : 0.0, cxb = ib <= ncols ? __ldg(&mult.cx[ib]) : 0.0;
+            double cyv[NIT];
+#pragma unroll
+            for (int k = 0; k < NIT; ++k) {
+                const int jj = 1 + t + k * TPF;
+                cyv[k] = jj < D::MC ? __ldg(&mult.cy[jj]) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < NIT; ++k) {
+                const int jj = 1 + t + k * TPF;
+                if (jj >= D::MC) break;
+                C y = buf[D::idx(jj)];
+                y.x = (T)(y.x * ((ia <= ncols) ? mult.eval(cb, cxa, cyv[k]) : 0.0));
+                y.y = (T)(y.y * ((ib <= ncols) ? mult.eval(cb, cxb, cyv[k]) : 0.0));
+                buf[D::idx(jj)] = y;
+            }
+        } else {
+            for (int jj = 1 + t; jj < M; jj += TPF) {
+                C y = buf[D::idx(jj)];
+                y.x = (T)(y.x * ((ia <= ncols) ? mult(cb, ia, jj) : 0.0));
+                y.y = (T)(y.y * ((ib <= ncols) ? mult(cb, ib, jj) : 0.0));
+                buf[D::idx(jj)] = y;
+            }
         }
         __syncthreads();
     }
@@ -220,7 +287,7 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
 
 // X pass: row j of level b as one complex line z = Gamma + i rest.
 template <class D, int NG>
-__global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
+__global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
     xpass_trial_kernel(const typename D::Real *__restrict__ gam, const typename D::Real *__restrict__ rest,
                        typename D::Real *__restrict__ t1, typename D::Real *__restrict__ t2, long long bs, int ld,
                        PlanT<typename D::Real> pl, int nrows) {
@@ -238,10 +305,27 @@ __global__ void __launch_bounds__(D::TPF *NG, 512 / (D::TPF * NG))
     const int j = blockIdx.x * NG + g + 1;
     const bool valid = j <= nrows;
     const long long row = b * bs + (long long)ld * (j - 1);
-    for (int i = t; i <= M; i += TPF) {
-        C z = Cx<T>::make(0, 0);
-        if (valid && i >= 1 && i < M) z = Cx<T>::make(gam[row + i - 1], rest[row + i - 1]);
-        buf[D::idx(i)] = z;
+    if constexpr (D::MC > 0) {
+        constexpr int NIT = (D::MC + 1 + TPF - 1) / TPF;
+        T za[NIT], zb[NIT];
+#pragma unroll
+        for (int k = 0; k < NIT; ++k) {
+            const int i = t + k * TPF;
+            const bool ok = valid && i >= 1 && i < D::MC;
+            za[k] = ok ? gam[row + i - 1] : (T)0;
+            zb[k] = ok ? rest[row + i - 1] : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NIT; ++k) {
+            const int i = t + k * TPF;
+            if (i <= D::MC) buf[D::idx(i)] = Cx<T>::make(za[k], zb[k]);
+        }
+    } else {
+        for (int i = t; i <= M; i += TPF) {
+            C z = Cx<T>::make(0, 0);
+            if (valid && i >= 1 && i < M) z = Cx<T>::make(gam[row + i - 1], rest[row + i - 1]);
+            buf[D::idx(i)] = z;
+        }
     }
     __syncthreads();
     D::dst(buf, pl, t, wt);
@@ -277,6 +361,31 @@ __global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
     const int c0 = blockIdx.x * W;  // 0-based first column
     const T *s1 = t1 + b * bs, *s2 = t2 + b * bs;
     T *dst = out + b * bs;
+    if constexpr (D::MC > 0) {
+        constexpr int NT = NG * TPF;
+        constexpr int NIT = (W * (D::MC + 1) + NT - 1) / NT;
+        constexpr int CH = 8;
+#pragma unroll
+        for (int k0 = 0; k0 < NIT; k0 += CH) {
+            T va[CH], vb[CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = threadIdx.x + (k0 + k) * NT;
+                const int c = e % W, jj = e / W;
+                const int col = c0 + c;
+                const bool ok = k0 + k < NIT && jj >= 1 && jj < D::MC && col < ncols;
+                const long long o = col + (long long)ncols * (jj - 1);
+                va[k] = ok ? s1[o] : (T)0;
+                vb[k] = ok ? s2[o] : (T)0;
+            }
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = threadIdx.x + (k0 + k) * NT;
+                const int c = e % W, jj = e / W;
+                if (k0 + k < NIT && jj <= D::MC) smem[c * G + D::idx(jj)] = Cx<T>::make(va[k], vb[k]);
+            }
+        }
+    } else
     for (int e = threadIdx.x; e < W * (M + 1); e += blockDim.x) {
         const int c = e % W, jj = e / W;
         const int col = c0 + c;
@@ -298,14 +407,30 @@ __global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
         const int col1 = c0 + c + 1;  // 1-based column
         const bool ok = col1 <= ncols;
         const double cxv = ok ? __ldg(&mult.cx[col1]) : 0.0;
-        for (int jj = 1 + t; jj < M; jj += TPF) {
+        auto combine = [&](int jj, double cyj) {
             const C y = buf[D::idx(jj)];
             double v = 0.0;
             if (ok) {
-                const double lam = -2 * ((cxv + __ldg(&mult.cy[jj])) - 2);
+                const double lam = -2 * ((cxv + cyj) - 2);
                 v = ((double)y.x * (1 - lam * cb) + (double)y.y) * (scale * recip(1 + lam * cb));
             }
             buf[D::idx(jj)] = Cx<T>::make((T)v, 0);
+        };
+        if constexpr (D::MC > 0) {
+            constexpr int NIT = (D::MC - 1 + TPF - 1) / TPF;
+            double cyv[NIT];
+#pragma unroll
+            for (int k = 0; k < NIT; ++k) {
+                const int jj = 1 + t + k * TPF;
+                cyv[k] = jj < D::MC ? __ldg(&mult.cy[jj]) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < NIT; ++k) {
+                const int jj = 1 + t + k * TPF;
+                if (jj < D::MC) combine(jj, cyv[k]);
+            }
+        } else {
+            for (int jj = 1 + t; jj < M; jj += TPF) combine(jj, __ldg(&mult.cy[jj]));
         }
         __syncthreads();
     }
@@ -410,9 +535,9 @@ __global__ void nonlinear_kernel(NonlinArgs<T> a) {
 // A 2D grid over the faces: blockIdx.y < ceil((ny+1)/by) covers the x faces
 // (rows j <= ny) and, offset by that count, the y faces (rows j <= ny+1).
 // Batch b (blockIdx.z) uses psi + b*bs, q + b*qbs, coarse + b*cbs.
-template <class T>
-__global__ void curl_kernel(T *__restrict__ qout, long long qbs, const T *__restrict__ psi, long long bs,
-                            const T *__restrict__ coarse, long long cbs, Grid g) {
+template <class T, class TP, class TC>
+__global__ void curl_kernel(T *__restrict__ qout, long long qbs, const TP *__restrict__ psi, long long bs,
+                            const TC *__restrict__ coarse, long long cbs, Grid g) {
     const int nx = g.nx, ny = g.ny;
     const long long nu = (long long)(nx + 1) * ny;
     const int rows_u = (ny + blockDim.y - 1) / blockDim.y;
@@ -420,8 +545,8 @@ __global__ void curl_kernel(T *__restrict__ qout, long long qbs, const T *__rest
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = (yface ? blockIdx.y - rows_u : blockIdx.y) * blockDim.y + threadIdx.y + 1;
     const int b = blockIdx.z;
-    const T *Pt = psi + b * bs;
-    const T *C = coarse ? coarse + b * cbs : nullptr;
+    const TP *Pt = psi + b * bs;
+    const TC *C = coarse ? coarse + b * cbs : nullptr;
     T *q = qout + b * qbs;
     auto P = [&](long long k) -> double { return (double)Pt[k]; };
     if (!yface) {
