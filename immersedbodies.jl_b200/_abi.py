@@ -77,6 +77,8 @@ EXPORTS = {
     "ibpm_diag_binv": (C.c_int, [C.c_void_p, _dp]),
     "ibpm_diag_vort2flux": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "ibpm_diag_reg": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "ibpm_lap_inv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ibpm_noalloc_last_error": (C.c_char_p, []),
 }
 KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3}
 

@@ -1,8 +1,9 @@
 """Builds libibpm_b200.so in-tree for sm_100a (nvcc, no JIT cache).
 
-Two translation units: ibpm.cu (transforms, stencils, host runtime and C ABI)
-and coupling.cu, compiled with -fmad=false so the regularised-delta weights
-and the E / E^T sums round exactly like the reference (no fused multiply-add).
+Translation units: ibpm.cu (transforms, stencils, host runtime and C ABI);
+coupling.cu, compiled with -fmad=false so the regularised-delta weights and the
+E / E^T sums round exactly like the reference (no fused multiply-add); and
+noalloc.cu (the allocation-free Laplacian-inverse entry point).
 """
 from __future__ import annotations
 
@@ -17,7 +18,7 @@ OUT = os.path.join(HERE, "lib", "libibpm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "550"]
-UNITS = [("ibpm.cu", []), ("coupling.cu", ["-fmad=false"])]
+UNITS = [("ibpm.cu", []), ("coupling.cu", ["-fmad=false"]), ("noalloc.cu", [])]
 
 
 def _deps():

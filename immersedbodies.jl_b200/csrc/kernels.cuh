@@ -601,7 +601,7 @@ __global__ void coarsify_kernel(T *__restrict__ coarse, const T *__restrict__ fi
 // x = Binv z for the precomputed B^-1 (src/coupling.jl:187-192), column-major n x n.
 // Grid (ceil(n/64), ceil(n/64)); partial sums part[chunk * n + row], summed in
 // chunk order by binv_reduce_kernel (deterministic).
-__global__ void __launch_bounds__(256) binv_gemv_kernel(const double *__restrict__ A, const double *__restrict__ z,
+static __global__ void __launch_bounds__(256) binv_gemv_kernel(const double *__restrict__ A, const double *__restrict__ z,
                                                         double *__restrict__ part, int n) {
     __shared__ double red[4][64];
     const int r = threadIdx.x % 64, s = threadIdx.x / 64;
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(256) binv_gemv_kernel(const double *__restrict
 
 // F~b = sum of the chunk partials; update_vars! fb = F~b h / dt (problem.jl:676-685);
 // total force sum over panels (problem.jl:853-856).  One block.
-__global__ void binv_reduce_kernel(const double *__restrict__ part, int nchunk, int n, double *__restrict__ fbt,
+static __global__ void binv_reduce_kernel(const double *__restrict__ part, int nchunk, int n, double *__restrict__ fbt,
                                    double *__restrict__ fb, double *__restrict__ total, double h, double dt,
                                    int from_part) {
     __shared__ double sx[32], sy[32];
@@ -663,7 +663,7 @@ __global__ void binv_reduce_kernel(const double *__restrict__ part, int nchunk, 
 // In-place Gauss-Jordan inversion of a symmetric positive definite matrix
 // (stands in for LinearAlgebra.inv at src/coupling.jl:190).  Step k, part 1:
 // save the pivot row/column.
-__global__ void gj_save_kernel(const double *__restrict__ A, int n, int k, double *__restrict__ rowk,
+static __global__ void gj_save_kernel(const double *__restrict__ A, int n, int k, double *__restrict__ rowk,
                                double *__restrict__ colk, int *err) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
@@ -673,7 +673,7 @@ __global__ void gj_save_kernel(const double *__restrict__ A, int n, int k, doubl
     colk[t] = A[t + (long long)n * k];
 }
 // part 2: rank-1 update of every element
-__global__ void gj_update_kernel(double *__restrict__ A, int n, int k, const double *__restrict__ rowk,
+static __global__ void gj_update_kernel(double *__restrict__ A, int n, int k, const double *__restrict__ rowk,
                                  const double *__restrict__ colk) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
@@ -692,7 +692,7 @@ __global__ void gj_update_kernel(double *__restrict__ A, int n, int k, const dou
 }
 
 // Identity columns [c0, c0+nb) of a 2np-length basis, one per batch.
-__global__ void unit_columns_kernel(double *__restrict__ f, int n, int c0, int nb) {
+static __global__ void unit_columns_kernel(double *__restrict__ f, int n, int c0, int nb) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n * nb) return;
     const int b = t / n, k = t % n;

@@ -3,7 +3,7 @@
  * ImmersedBodies.jl's CNAB/IBPM time step.
  *
  * The entry points are what a Julia `AbstractSolver` (src/solver.jl:6-28)
- * binds with `ccall`; see INTEGRATION.md for the Julia and Python stubs.
+ * binds with `ccall` (the module immersedbodies.jl_b200/julia/ImmersedBodiesCUDA.jl).
  *
  *   reference interface                         replaced by
  *   ------------------------------------------  -------------------------------
@@ -171,6 +171,21 @@ int ibpm_diag_vort2flux(ibpm_handle *h, double *gamma, double *psi, double *q);
 /* rot!(reg!(f)) (fluid.jl:101-111 after coupling.jl:72-85) into gamma1 (ng), and
  * regT!(f, q1) (coupling.jl:57-69) from a level-1 flux q1 (nq); NULL skips either. */
 int ibpm_diag_reg(ibpm_handle *h, const double *f, double *gamma1, const double *q1, double *fout);
+
+/* Laplacian-inverse solve x = Δ⁻¹ b (the operator of src/fluid.jl:117-119) for callers
+ * that cannot allocate device memory.  No counterpart in the reference: it exists
+ * for code running inside another framework's memory pool or a fixed arena, or a
+ * host loop that must not allocate between steps.  b and x are caller-owned
+ * device buffers of (nx-1) x (ny-1) doubles, column-major; x may not alias b.
+ * The scratch fields and transform tables live in one static device array of
+ * about 4.3 MB that each GPU loading the library keeps until exit; it limits
+ * (nx-1)(ny-1) to 262144 cells (nx, ny even, <= 1024, of the form 2^a 3^b 5^c).
+ * Larger sizes return IBPM_ERR_INVALID.  The first call on a device writes the
+ * tables (make it before any stream capture); all calls share the array, so
+ * calls that overlap on the GPU race.  stream is a cudaStream_t (NULL: default).
+ * On error ibpm_noalloc_last_error() gives the message. */
+int ibpm_lap_inv_noalloc(int nx, int ny, const double *b, double *x, void *stream);
+const char *ibpm_noalloc_last_error(void);
 
 #ifdef __cplusplus
 }
