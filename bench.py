@@ -17,6 +17,7 @@ import argparse
 import importlib.util
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -41,6 +42,34 @@ def load_package():
     sys.modules[name] = mod
     spec.loader.exec_module(mod)
     return mod
+
+
+def step_bytes_model(nx: int, ny: int, L: int, npanel: int, s: float = 1.0) -> float:
+    """Algorithmic HBM bytes of one static-body step: one read and one write of every
+    field each pass touches, with each 2D DST-diagonalised solve counted as three
+    full passes.  G, Q are one level of circulation / flux in bytes.
+
+    nonlinear + rhs L(Q+4G); A and Ainv solves 12GL; two vort2flux
+    2(6GL + L(G+Q) + 1.25G(L-1)); projection 6G + 2GL; B^-1 matvec 8(2np)^2."""
+    G = 8.0 * (nx - 1) * (ny - 1) * s
+    Q = 8.0 * ((nx + 1) * ny + nx * (ny + 1)) * s
+    return (L * (Q + 4 * G) + 12 * G * L + 2 * (6 * G * L + L * (G + Q) + 1.25 * G * (L - 1)) + 6 * G + 2 * G * L
+            + 8.0 * (2 * npanel) ** 2)
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from its committed ncu summary (a line
+    `traffic_bytes_per_launch: N`), or None when no summary exists."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_cylinder_re100_1024.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                m = re.match(r"\s*traffic_bytes_per_launch:\s*([0-9.eE+]+)", line)
+                if m:
+                    return float(m.group(1)), os.path.relpath(path, ROOT)
+    except OSError:
+        pass
+    return None, None
 
 
 def read_peaks():
@@ -243,20 +272,27 @@ def main():
     prof_steps = max(2, min(args.steps, 10))
     solver.profile(True)
     solver.advance_many(prof_steps)
-    kern = {k: solver.profile_read(k) for k in ("ypass", "xpass", "nonlinear", "curl")}
+    kern = {k: solver.profile_read(k) for k in ("ypass", "xpass", "nonlinear", "curl", "xtrial", "ytrial")}
     solver.profile(False)
 
     peak, peak_kind = read_peaks()
     n_y, ms_y, b_y = kern["ypass"]
-    dom = "ypass_kernel (DST along y, spectral multiply, DST along y)"
+    dom = "ypass_kernel (one level: DST along y, multiply by scale/Λ, DST along y)"
     achieved = (b_y / n_y) / ((ms_y / n_y) / 1000.0) / 1e9 if n_y else None
+    traffic, traffic_src = read_traffic("ypass_kernel")
+    step_bytes = step_bytes_model(nx, ny, L, prob.bodies.npanel)
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "traffic": None, "peak_source": peak_kind,
+                "frac": achieved / peak if achieved else None, "traffic": traffic,
+                "traffic_source": traffic_src and f"dram__bytes_read.sum + dram__bytes_write.sum, ncu ({traffic_src})",
+                "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": b_y / n_y if n_y else None,
                 "launch_ms": ms_y / n_y if n_y else None,
                 "kernel_ms_per_step": {k: v[1] / prof_steps for k, v in kern.items()},
                 "timing": f"CUDA events around each launch during {prof_steps} profiled steps (eager launches) "
-                          "after the timed region"}
+                          "after the timed region",
+                "step": {"algorithmic_bytes": step_bytes, "achieved": step_bytes / (ms_step / 1000.0) / 1e9,
+                         "frac": step_bytes / (ms_step / 1000.0) / 1e9 / peak, "unit": "GB/s",
+                         "model": "one read + one write of each field per pass; 3 passes per 2D solve"}}
 
     # the mixed-precision engine on the same case, stepped to the same index
     chosen = None
@@ -290,9 +326,11 @@ def main():
         try:
             threads = os.cpu_count() or 1
             v, used = cpu_time_oracle(ib, 3, 1, threads)
+            v1, _ = cpu_time_oracle(ib, 1, 0, 1)
             cpu = {"value": v, "unit": "steps/s", "cores": used, "kind": "port",
                    "sample": "3 steps of the same 1024^2 x 5 case after 1 warm-up step, all host threads; "
-                             "CPU FP64 restatement of the reference (Julia is not installed); B^-1 setup skipped"}
+                             "CPU FP64 restatement of the reference (Julia is not installed); B^-1 setup skipped",
+                   "single_thread": {"value": v1, "unit": "steps/s", "cores": 1, "sample": "1 step, no warm-up"}}
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "error": str(e)}
 

@@ -80,7 +80,7 @@ EXPORTS = {
     "ibpm_lap_inv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ibpm_noalloc_last_error": (C.c_char_p, []),
 }
-KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3}
+KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5}
 
 _lib = None
 

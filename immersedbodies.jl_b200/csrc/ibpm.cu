@@ -300,7 +300,7 @@ struct Engine final : ibpm_handle {
             const int pe = prof_begin();
             xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1, t2, ng, nx - 1, plx, ny - 1);
             check_launch();
-            prof_end(pe, IBPM_KCLASS_XPASS, 32.0 * (double)ng * L);
+            prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(T) * (double)ng * L);
         }
         {
             const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), L);
@@ -316,7 +316,7 @@ struct Engine final : ibpm_handle {
             ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1, t2, rhs, ng, nx - 1, ply,
                                                                        mult(MULT_AIMPL, 1, 1));
             check_launch();
-            prof_end(pe, IBPM_KCLASS_YPASS, 24.0 * (double)ng * L);
+            prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(T) * (double)ng * L);
         }
         xpass(in_plain(rhs, ng), out_plain(Gnew, ng), L);
     }

@@ -151,7 +151,9 @@ int64_t ibpm_kernel_launches(const ibpm_handle *h);
 #define IBPM_KCLASS_YPASS 1         /* DST along y, spectral multiply, DST along y */
 #define IBPM_KCLASS_NONLINEAR 2     /* nonlinear advection term */
 #define IBPM_KCLASS_CURL 3          /* curl of the streamfunction */
-#define IBPM_KCLASS_COUNT 4
+#define IBPM_KCLASS_XTRIAL 4        /* trial solve, first X pass (all levels) */
+#define IBPM_KCLASS_YTRIAL 5        /* trial solve, Y pass with the A/Ainv multiplies (all levels) */
+#define IBPM_KCLASS_COUNT 6
 int ibpm_profile(ibpm_handle *h, int enable);
 int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms, double *bytes);
 
