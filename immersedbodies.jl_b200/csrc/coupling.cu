@@ -182,28 +182,39 @@ __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *
 // regT! (src/coupling.jl:57-69): fb[p, c] = dot(q_c[7x7 at p], w[p, c]) in
 // column-major order.  With add_q0 it is couple_surface_rigid's
 // Ftmp = E (qs + q0) - ub h (src/coupling.jl:239-244).
+// One warp per output: the lanes form the 49 products w q of the support in
+// parallel; lane 0 adds them in the reference's order (column-major over the
+// support, from 0), so the sum rounds as a sequential dot product.
+constexpr int kRegTWarps = 4;
 template <class T>
-__global__ void regT_kernel(Panels P, const T *__restrict__ q, long long qbs, double *__restrict__ out,
-                            long long obs, int nbatch, int add_q0, const StepDev *__restrict__ prm, Grid g) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32 * kRegTWarps) regT_kernel(Panels P, const T *__restrict__ q, long long qbs,
+                                                                double *__restrict__ out, long long obs, int nbatch,
+                                                                int add_q0, const StepDev *__restrict__ prm, Grid g) {
+    __shared__ double prod[kRegTWarps][49];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * kRegTWarps + wid;
     const int np = P.np;
-    if (t >= 2 * np * nbatch) return;
+    if (t >= 2 * np * nbatch) return;  // the whole warp leaves together
     const int b = t / (2 * np), pcomp = t % (2 * np);
     const int c = pcomp / np, p = pcomp % np;
     const long long nu = (long long)(g.nx + 1) * g.ny;
     const T *Q = q + b * qbs;
     const int i0 = P.pc[2 * p] - 3, j0 = P.pc[2 * p + 1] - 3;
     const double *w = P.w + (long long)(p * 2 + c) * 49;
-    double s = 0.0;
-    for (int bb = 0; bb < 7; ++bb)
-        for (int a = 0; a < 7; ++a) {
-            const int i = i0 + a, j = j0 + bb;
-            double v = c == 0 ? (double)Q[UI(i, j)] : (double)Q[VI(i, j)];
-            if (add_q0) v = v + (c == 0 ? base_flux_x(g, prm, 1, i, j) : base_flux_y(g, prm, 1, i, j));
-            s += v * w[bb * 7 + a];
-        }
-    if (add_q0) s = s - P.ub[c * np + p] * g.h;
-    out[b * obs + c * np + p] = s;
+    for (int k = lane; k < 49; k += 32) {
+        const int bb = k / 7, a = k % 7;
+        const int i = i0 + a, j = j0 + bb;
+        double v = c == 0 ? (double)Q[UI(i, j)] : (double)Q[VI(i, j)];
+        if (add_q0) v = v + (c == 0 ? base_flux_x(g, prm, 1, i, j) : base_flux_y(g, prm, 1, i, j));
+        prod[wid][k] = v * w[k];
+    }
+    __syncwarp();
+    if (lane == 0) {
+        double s = 0.0;
+        for (int k = 0; k < 49; ++k) s += prod[wid][k];
+        if (add_q0) s = s - P.ub[c * np + p] * g.h;
+        out[b * obs + c * np + p] = s;
+    }
 }
 
 // _update!(panels, ::MovingRigidBody, t) (src/bodies.jl:12-31) for panels [p0, p1)
@@ -238,7 +249,8 @@ template <class T>
 void launch_regT(const Panels &P, const T *q, long long qbs, double *out, long long obs, int nbatch, int add_q0,
                  const StepDev *prm, const Grid &g, cudaStream_t st) {
     const int nt = 2 * P.np * nbatch;
-    regT_kernel<T><<<(nt + 127) / 128, 128, 0, st>>>(P, q, qbs, out, obs, nbatch, add_q0, prm, g);
+    regT_kernel<T><<<(nt + kRegTWarps - 1) / kRegTWarps, 32 * kRegTWarps, 0, st>>>(P, q, qbs, out, obs, nbatch,
+                                                                                  add_q0, prm, g);
 }
 template void launch_reg_patch<double>(const Panels &, const double *, long long, double *, long long, int,
                                        const Grid &, cudaStream_t);

@@ -919,7 +919,7 @@ void Engine<T>::step_body() {
     // only read the previous step's Gamma and q.
     {
         NonlinArgs<T> a{q, Gold, N1, N2, rest, prm, g};
-        const dim3 blk(32, 8), grd((nx - 1 + 31) / 32, (ny - 1 + 7) / 8, L);
+        const dim3 blk(kNlTX, kNlBY), grd((nx - 1 + kNlTX - 1) / kNlTX, (ny - 1 + kNlTY - 1) / kNlTY, L);
         const int pe = prof_begin();
         nonlinear_kernel<<<grd, blk, 0, st>>>(a);
         check_launch();

@@ -482,52 +482,104 @@ __device__ __forceinline__ double avg_qy(const NonlinArgs<T> &a, const T *q, lon
             base_flux_y(g, a.prm, lev, i - 1, j)) / 2;
 }
 
+// Tile of the nonlinear kernel: kNlTX x kNlTY circulation points per block of
+// kNlTX x kNlBY threads (two rows of outputs per thread).
+constexpr int kNlTX = 32, kNlTY = 16, kNlBY = 8;
+
+// nonlinear (src/fluid.jl:340-455) fused with the rhs assembly of
+// get_trial_state (src/fluid.jl:487-493), all levels (blockIdx.z) at once.
+// Every face average Q = (q + q0) pair sum / 2 (avg_flux!) and every Gamma of the
+// tile and its one-point halo is read once into shared memory; each flux product
+// (direct_product_loops!) and the rot! difference are then formed from there, with
+// the reference's expressions, so each value rounds exactly as in a direct
+// evaluation.
 template <class T>
-__global__ void nonlinear_kernel(NonlinArgs<T> a) {
+__global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a) {
     const Grid &g = a.g;
     const int nx = g.nx, ny = g.ny;
-    const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int b = blockIdx.z, lev = b + 1;
-    if (I > nx - 1 || J > ny - 1) return;
+    const int I0 = blockIdx.x * kNlTX, J0 = blockIdx.y * kNlTY;  // outputs I0+1..I0+TX, J0+1..J0+TY
     const long long nq = (long long)(nx + 1) * ny + (long long)nx * (ny + 1), ng = (long long)(nx - 1) * (ny - 1);
     const long long nu = (long long)(nx + 1) * ny;
     const T *q = a.q + b * nq;
     const T *Gt = a.gam + b * ng;
     const T *C = lev < g.L ? a.gam + (b + 1) * ng : nullptr;
-    auto G = [&](long long k) -> double { return (double)Gt[k]; };
-    // x-flux product at (i, j), i in 2..nx  (direct_product_loops!, fluid.jl:396-415)
-    auto fqx = [&](int i, int j) -> double {
-        if (j == 1)
-            return (avg_qy(a, q, nu, lev, i, 2) * G(GI(i - 1, 1)) +
-                    avg_qy(a, q, nu, lev, i, 1) * (getbc(C, g, SIDE_B, i) * 0.25)) / 2;
-        if (j == ny)
-            return (avg_qy(a, q, nu, lev, i, ny) * G(GI(i - 1, ny - 1)) +
-                    avg_qy(a, q, nu, lev, i, ny + 1) * (getbc(C, g, SIDE_T, i) * 0.25)) / 2;
-        return (avg_qy(a, q, nu, lev, i, j + 1) * G(GI(i - 1, j)) + avg_qy(a, q, nu, lev, i, j) * G(GI(i - 1, j - 1))) / 2;
-    };
-    // y-flux product at (i, j), j in 2..ny  (fluid.jl:417-436)
-    auto fqy = [&](int i, int j) -> double {
-        if (i == 1)
-            return -(avg_qx(a, q, lev, 2, j) * G(GI(1, j - 1)) + avg_qx(a, q, lev, 1, j) * (getbc(C, g, SIDE_L, j) * 0.25)) / 2;
-        if (i == nx)
-            return -(avg_qx(a, q, lev, nx, j) * G(GI(nx - 1, j - 1)) +
-                     avg_qx(a, q, lev, nx + 1, j) * (getbc(C, g, SIDE_R, j) * 0.25)) / 2;
-        return -(avg_qx(a, q, lev, i + 1, j) * G(GI(i, j - 1)) + avg_qx(a, q, lev, i, j) * G(GI(i - 1, j - 1))) / 2;
-    };
-    // rot! at Gamma(I, J) with i = I+1, j = J+1 (fluid.jl:106-108)
-    const double r = (fqx(I + 1, J) - fqx(I + 1, J + 1)) + (fqy(I + 1, J + 1) - fqy(I, J + 1));
+    __shared__ double aqy[kNlTY + 2][kNlTX];      // avg_qy(i, j), i = I0+2+x, j = J0+1+y
+    __shared__ double aqx[kNlTY][kNlTX + 2];      // avg_qx(i, j), i = I0+1+x, j = J0+2+y
+    __shared__ double gm[kNlTY + 2][kNlTX + 2];   // Gamma(i, j),  i = I0+x,   j = J0+y
+    const int tid = threadIdx.y * kNlTX + threadIdx.x;
+    constexpr int NT = kNlTX * kNlBY;
     const double hc = gridstep(g, lev);
-    const double n1 = r * (1 / (hc * hc));
-    a.out[b * ng + GI(I, J)] = (T)n1;
-    if (a.rest) {
-        // rest = dt b1 N1 + dt b2 N2 + rhsbc (fluid.jl:487-493), rhsbc = apply_bc!(0, get_bc(..); fac)
-        double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * (double)a.n2[b * ng + GI(I, J)];
-        if (lev < g.L && on_ring(g, I, J)) {
-            const double fac = 0.25 * g.dt / (g.Re * (hc * hc));
-            v = v + apply_bc_at(0.0, C, g, I, J, fac);
+    // base_flux! of a static grid is U hc on every face (fluid.jl:22-32)
+    const double sbx = a.prm->fs[0] * hc, sby = a.prm->fs[1] * hc;
+    const bool moving = g.grid_moving;
+#pragma unroll
+    for (int e = tid; e < (kNlTY + 2) * kNlTX; e += NT) {
+        const int x = e % kNlTX, y = e / kNlTX;
+        const int i = I0 + 2 + x, j = J0 + 1 + y;
+        double v = 0.0;
+        if (i <= nx && j <= ny + 1) {
+            if (moving)
+                v = avg_qy(a, q, nu, lev, i, j);
+            else
+                v = ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + sby + sby) / 2;
         }
-        a.rest[b * ng + GI(I, J)] = (T)v;
+        aqy[y][x] = v;
+    }
+#pragma unroll
+    for (int e = tid; e < kNlTY * (kNlTX + 2); e += NT) {
+        const int x = e % (kNlTX + 2), y = e / (kNlTX + 2);
+        const int i = I0 + 1 + x, j = J0 + 2 + y;
+        double v = 0.0;
+        if (i <= nx + 1 && j <= ny) {
+            if (moving)
+                v = avg_qx(a, q, lev, i, j);
+            else
+                v = ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + sbx + sbx) / 2;
+        }
+        aqx[y][x] = v;
+    }
+#pragma unroll
+    for (int e = tid; e < (kNlTY + 2) * (kNlTX + 2); e += NT) {
+        const int x = e % (kNlTX + 2), y = e / (kNlTX + 2);
+        const int i = I0 + x, j = J0 + y;
+        gm[y][x] = (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1) ? (double)Gt[GI(i, j)] : 0.0;
+    }
+    __syncthreads();
+    const int x = threadIdx.x, I = I0 + 1 + x;
+    if (I > nx - 1) return;
+    // x-flux product at (I+1, j) (direct_product_loops!, fluid.jl:396-415)
+    auto fqx = [&](int j) -> double {
+        const int i = I + 1, yj = j - J0;
+        if (j == 1) return (aqy[yj][x] * gm[yj][x + 1] + aqy[yj - 1][x] * (getbc(C, g, SIDE_B, i) * 0.25)) / 2;
+        if (j == ny) return (aqy[yj - 1][x] * gm[yj - 1][x + 1] + aqy[yj][x] * (getbc(C, g, SIDE_T, i) * 0.25)) / 2;
+        return (aqy[yj][x] * gm[yj][x + 1] + aqy[yj - 1][x] * gm[yj - 1][x + 1]) / 2;
+    };
+    // y-flux product at (i, J+1), i in {I, I+1} (fluid.jl:417-436)
+    auto fqy = [&](int i, int y) -> double {
+        const int xi = i - I0;  // aqx column of avg_qx(i, .) is xi - 1, gm column of Gamma(i, .) is xi
+        if (i == 1) return -(aqx[y][xi] * gm[y + 1][xi] + aqx[y][xi - 1] * (getbc(C, g, SIDE_L, J0 + 2 + y) * 0.25)) / 2;
+        if (i == nx)
+            return -(aqx[y][xi - 1] * gm[y + 1][xi - 1] + aqx[y][xi] * (getbc(C, g, SIDE_R, J0 + 2 + y) * 0.25)) / 2;
+        return -(aqx[y][xi] * gm[y + 1][xi] + aqx[y][xi - 1] * gm[y + 1][xi - 1]) / 2;
+    };
+#pragma unroll
+    for (int k = 0; k < kNlTY / kNlBY; ++k) {
+        const int y = threadIdx.y + k * kNlBY, J = J0 + 1 + y;
+        if (J > ny - 1) break;
+        // rot! at Gamma(I, J) with i = I+1, j = J+1 (fluid.jl:106-108)
+        const double r = (fqx(J) - fqx(J + 1)) + (fqy(I + 1, y) - fqy(I, y));
+        const double n1 = r * (1 / (hc * hc));
+        a.out[b * ng + GI(I, J)] = (T)n1;
+        if (a.rest) {
+            // rest = dt b1 N1 + dt b2 N2 + rhsbc (fluid.jl:487-493), rhsbc = apply_bc!(0, get_bc(..); fac)
+            double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * (double)a.n2[b * ng + GI(I, J)];
+            if (lev < g.L && on_ring(g, I, J)) {
+                const double fac = 0.25 * g.dt / (g.Re * (hc * hc));
+                v = v + apply_bc_at(0.0, C, g, I, J, fac);
+            }
+            a.rest[b * ng + GI(I, J)] = (T)v;
+        }
     }
 }
 
@@ -609,7 +661,12 @@ static __global__ void __launch_bounds__(256) binv_gemv_kernel(const double *__r
     const int cbeg = blockIdx.y * 64;
     double acc = 0.0;
     if (row < n) {
-        for (int c = cbeg + s; c < min(cbeg + 64, n); c += 4) acc += A[row + (long long)n * c] * __ldg(&z[c]);
+        if (cbeg + 64 <= n) {
+#pragma unroll
+            for (int c = cbeg + s; c < cbeg + 64; c += 4) acc += A[row + (long long)n * c] * __ldg(&z[c]);
+        } else {
+            for (int c = cbeg + s; c < n; c += 4) acc += A[row + (long long)n * c] * __ldg(&z[c]);
+        }
     }
     red[s][r] = acc;
     __syncthreads();
