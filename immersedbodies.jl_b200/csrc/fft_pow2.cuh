@@ -238,6 +238,55 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t
     __syncthreads();
 }
 
+// The first Stockham stage (stride 1) with the DST pre-twiddle folded into its
+// reads: input n is v_n = s (z_n + z_{M-n}) + (z_n - z_{M-n}) / 2 with
+// s = sin(pi min(n, M-n) / M), v_0 = 0 -- the values the separate pre-twiddle
+// pass writes, formed in registers from z_n and its mirror.  buf[0..M] hold z
+// (z_0 = z_M = 0).
+template <int M, int R, int TPF, class C, class T>
+__device__ __forceinline__ void stage_first_pre(C *buf, const T *__restrict__ sn, int t) {
+    constexpr int NB = M / R;
+    constexpr int K = NB >= TPF ? NB / TPF : 1;
+    constexpr bool ALL = NB >= TPF;
+    constexpr int H = M / 2;
+    static_assert((NB % TPF == 0 || TPF % NB == 0) && NB % 16 == 0, "stage layout");
+    constexpr int RSTEP = NB * 17 / 16;
+    T s[K][R];
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {  // table loads first
+        const int j = t + kb * TPF;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int n = j + r * NB;
+            s[kb][r] = (ALL || j < NB) ? __ldg(&sn[n <= H ? n : M - n]) : (T)0;
+        }
+    }
+    C v[K][R];
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (!ALL && j >= NB) break;
+        const C *src = buf + pad16(j);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int n = j + r * NB;
+            const C a = src[r * RSTEP], b = buf[pad16(M - n)];
+            v[kb][r] = n == 0 ? Cx<T>::make(0, 0) : s[kb][r] * (a + b) + (T)0.5 * (a - b);
+        }
+        DftC<R, C>::run(v[kb]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (!ALL && j >= NB) break;
+        C *dst = buf + pad16(j * R);
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[write_off<R, 1>(r)] = v[kb][r];
+    }
+    __syncthreads();
+}
+
 template <int M, class T, class PL = Pow2Plan<M>>
 struct Pow2Dst {
     using P = PL;
@@ -346,9 +395,19 @@ struct Pow2Dst {
         __syncthreads();
     }
 
+    // the FFT of the pre-twiddled packed lines, the pre-twiddle folded into stage 1
+    static __device__ __forceinline__ void fft_pre(C *buf, const C *__restrict__ tw, const T *__restrict__ sn, int t) {
+        constexpr int N1 = P::R0, N2 = N1 * P::R1, N3 = N2 * P::R2, N4 = N3 * P::R3;
+        static_assert(N4 * P::R4 == M, "plan must factor M");
+        stage_first_pre<M, P::R0, TPF, C, T>(buf, sn, t);
+        stage_ct<M, P::R1, N1, TPF, C>(buf, tw, t);
+        stage_ct<M, P::R2, N2, TPF, C>(buf, tw, t);
+        if constexpr (P::R3 > 1) stage_ct<M, P::R3, N3, TPF, C>(buf, tw, t);
+        if constexpr (P::R4 > 1) stage_ct<M, P::R4, N4, TPF, C>(buf, tw, t);
+    }
+
     static __device__ __forceinline__ void dst(C *buf, const PlanT<T> &pl, int t, double2 *wt) {
-        pre(buf, pl.sn, t);
-        fft(buf, pl.tw, t);
+        fft_pre(buf, pl.tw, pl.sn, t);
         post(buf, t, wt);
     }
 };
