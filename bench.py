@@ -167,6 +167,69 @@ def cpu_time_oracle(ib, steps: int, warmup: int, threads: int):
     return steps / dt, used
 
 
+def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int = 100):
+    """CG iterations and steps/s of the moving-body case (the 512^2 x 4-level
+    pitching and plunging plate, 101 points, Re 500, dt 0.002, CG to an absolute
+    residual of 1e-10) at a held-out reduced frequency k = 0.55, with the
+    reference's start (the previous solution), the extrapolated start and the
+    learned start; the network is trained on samples of k = 0.25, 0.45, 0.65 and
+    0.85 generated by the solver (after a 60-step start-up)."""
+    import torch
+
+    cg = dict(reltol=0.0, abstol=1e-10, maxiter=5000)
+
+    def make(k):
+        return ib.GpuCnabSolver(ib.State(ib.configs.pitching_plate(k)), cg=cg, device=device)
+
+    t0 = time.perf_counter()
+    X, T = ib.warmstart.make_training_set(make, (0.25, 0.45, 0.65, 0.85), train_steps, skip=60)
+    t_collect = time.perf_counter() - t0
+    net = ib.WarmStartNet(seed=2026, device=device)
+    net.fit_normalisation(X, T)
+    t0 = time.perf_counter()
+    losses = np.concatenate([net.train(X, T, epochs=200, batch=64, lr=1e-3),
+                             net.train(X, T, epochs=200, batch=64, lr=2e-4, seed=8)])
+    t_train = time.perf_counter() - t0
+    out = {}
+    for mode in ("previous", "extrapolated", "learned"):
+        s = make(0.55)
+        if mode != "previous":
+            s.set_warm_start(net if mode == "learned" else None, mode=mode)
+        for _ in range(60):  # start-up transient, excluded
+            s.advance_()
+        stream = torch.cuda.ExternalStream(s.stream_handle())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        it, r0, coef = [], [], []
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(eval_steps):
+            s.advance_()
+            inf = s.info()
+            it.append(inf.last_cg_iters)
+            r0.append(inf.first_cg_residual)
+            coef.append(list(inf.warm_start_coef))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[mode] = {"cg_iterations_mean": float(np.mean(it)), "first_residual_geomean": float(np.exp(np.mean(np.log(r0)))),
+                     "steps_per_s": eval_steps / (ms / 1000.0),
+                     "galerkin_coef_median": [float(v) for v in np.median(np.asarray(coef), axis=0)]}
+        if mode == "learned":
+            Xh, Th, _ = ib.warmstart.collect_samples(s, 30)
+            ph = net.forward(Xh)
+            out[mode]["held_out_r2"] = float(1 - ((ph - Th) ** 2).sum() / ((Th - Th.mean(axis=(0, 2), keepdims=True)) ** 2).sum())
+        del s
+    base = out["previous"]
+    return {"workload": "pitching_plate_512: 512x512 cells x 4 levels, 101-point plate pitching 30 deg and plunging "
+                        "0.25 chord, Re 500, dt 0.002; CG to |r| <= 1e-10; held-out k = 0.55",
+            "training": {"samples": int(X.shape[0]), "ks": [0.25, 0.45, 0.65, 0.85], "collect_s": t_collect,
+                         "train_s": t_train, "epochs": int(losses.size), "loss_first": float(losses[0]),
+                         "loss_last": float(losses[-1])},
+            "modes": out,
+            "iterations_vs_previous": {m: out[m]["cg_iterations_mean"] / base["cg_iterations_mean"] for m in out},
+            "steps_per_s_vs_previous": {m: out[m]["steps_per_s"] / base["steps_per_s"] for m in out}}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -195,6 +258,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-chosen", action="store_true", help="skip the mixed-precision engine")
+    ap.add_argument("--no-learned", action="store_true", help="skip the moving-body CG warm-start comparison")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
@@ -321,6 +385,8 @@ def main():
                   "bar": "|dC_D|,|dC_L| <= 1e-4 and vorticity rel-L2 <= 1e-5 vs FP64",
                   "meets_bar": bool(dC <= 1e-4 and vort <= 1e-5)}
 
+    learned = None if args.no_learned else warm_start_report(ib, local)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -345,7 +411,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps, "api": "GpuCnabSolver.advance_ (ctypes -> ibpm_advance + ibpm_get_forces)"},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-                "chosen_form": chosen}
+                "chosen_form": chosen, "learned_warm_start": learned}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

@@ -7,6 +7,7 @@ library through its C ABI (include/ibpm_b200.h).
 """
 from . import curves as Curves
 from . import configs
+from . import warmstart
 from .io import load_state, load_state_, save_state
 from .problem import (CNAB, Bodies, CartesianGrid, Fluid, GridIndices, GridVelocity, MovingGrid, MovingRigidBody,
                       MultiDomainGrid, Panels, PanelState, Problem, RigidBodyTransform, State, StaticBody,
@@ -14,5 +15,6 @@ from .problem import (CNAB, Bodies, CartesianGrid, Fluid, GridIndices, GridVeloc
                       inc_time_index_, n_panels, set_time_index_, timestep, update_vars_, vorticity, x_velocity,
                       y_velocity)
 from .solver import AbstractSolver, GpuCnabSolver, advance_, create_solver, getstate, solve, solve_
+from .warmstart import WarmStartNet
 
 __all__ = [n for n in dir() if not n.startswith("_")]

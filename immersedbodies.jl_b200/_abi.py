@@ -24,6 +24,7 @@ IBPM_FP64 = 0
 IBPM_FP32 = 1
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 _ip = C.POINTER(C.c_int32)
 
 
@@ -54,7 +55,8 @@ class ibpm_state_view(C.Structure):
 
 class ibpm_info(C.Structure):
     _fields_ = [("nq", C.c_int64), ("ng", C.c_int64), ("nbc", C.c_int64), ("static_bodies", C.c_int32),
-                ("last_cg_iters", C.c_int32), ("last_cg_residual", C.c_double), ("device_bytes", C.c_int64)]
+                ("last_cg_iters", C.c_int32), ("last_cg_residual", C.c_double), ("device_bytes", C.c_int64),
+                ("first_cg_residual", C.c_double), ("warm_start_coef", C.c_double * 2)]
 
 
 EXPORTS = {
@@ -77,9 +79,25 @@ EXPORTS = {
     "ibpm_diag_binv": (C.c_int, [C.c_void_p, _dp]),
     "ibpm_diag_vort2flux": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "ibpm_diag_reg": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "ibpm_net_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
+                                  C.POINTER(C.c_void_p)]),
+    "ibpm_net_destroy": (None, [C.c_void_p]),
+    "ibpm_net_num_params": (C.c_int64, [C.c_void_p]),
+    "ibpm_net_get_params": (C.c_int, [C.c_void_p, _fp]),
+    "ibpm_net_set_params": (C.c_int, [C.c_void_p, _fp]),
+    "ibpm_net_set_normalisation": (C.c_int, [C.c_void_p, _fp, _fp, _fp, _fp]),
+    "ibpm_net_get_normalisation": (C.c_int, [C.c_void_p, _fp, _fp, _fp, _fp]),
+    "ibpm_net_forward": (C.c_int, [C.c_void_p, _fp, C.c_int64, C.c_int32, _fp]),
+    "ibpm_net_loss_grad": (C.c_int, [C.c_void_p, _fp, _fp, C.c_int64, C.c_int32, _fp, _fp]),
+    "ibpm_net_train": (C.c_int, [C.c_void_p, _fp, _fp, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                 C.c_uint64, _fp]),
+    "ibpm_net_last_error": (C.c_char_p, [C.c_void_p]),
+    "ibpm_set_warm_start": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "ibpm_warm_start_sample": (C.c_int, [C.c_void_p, _fp, _fp, _fp]),
     "ibpm_lap_inv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ibpm_noalloc_last_error": (C.c_char_p, []),
 }
+IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED = 0, 1, 2
 KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5}
 
 _lib = None
@@ -121,3 +139,12 @@ def check(lib, h, rc: int):
         msg = lib.ibpm_last_error(h)
         raise IbpmError(rc, msg.decode() if msg else f"ibpm error {rc}")
     return rc
+
+
+def fptr(a):
+    """Pointer to a contiguous float32 numpy array (None -> NULL)."""
+    if a is None:
+        return None
+    if a.dtype != np.float32 or not a.flags.c_contiguous:
+        raise ValueError("expected a C-contiguous float32 array")
+    return a.ctypes.data_as(_fp)

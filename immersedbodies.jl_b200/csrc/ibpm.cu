@@ -23,6 +23,7 @@
 
 #include "../../include/ibpm_b200.h"
 #include "coupling.h"
+#include "warmstart.h"
 #include "kernels.cuh"
 
 using namespace ibpm;
@@ -119,6 +120,8 @@ struct ibpm_handle {
     virtual void diag_binv(double *out) = 0;
     virtual void diag_vort2flux(double *gamma, double *psi, double *q) = 0;
     virtual void diag_reg(const double *f, double *gamma1, const double *q1, double *fout) = 0;
+    virtual void set_warm_start(ibpm_net *net, int mode) = 0;
+    virtual void warm_start_sample(float *features, float *target, float *prediction) = 0;
 };
 
 template <class T>
@@ -155,6 +158,14 @@ struct Engine final : ibpm_handle {
     double *Fbt = nullptr, *fb = nullptr, *total = nullptr;
     StepDev *prm = nullptr, *prm_h = nullptr;
     double *motion = nullptr, *motion_h = nullptr;
+    // learned CG warm start (moving bodies): the installed network, the solution
+    // of two steps back, the features and prediction of the current step
+    ibpm_net *ws = nullptr;
+    int ws_mode = IBPM_WS_PREVIOUS;
+    double *Fprev = nullptr, *ws_z = nullptr, *ws_bz = nullptr, *ws_x2 = nullptr, *ws_bx2 = nullptr;
+    float *ws_feat = nullptr, *ws_y = nullptr, *ws_act = nullptr;
+    size_t ws_act_cap = 0;
+    int *pbody_d = nullptr;
     double fs_last[2] = {0, 0}, gm_last[6] = {0, 0, 0, 0, 0, 0};
     // work
     int kbatch = 1;  // columns per batch in the B setup
@@ -168,7 +179,7 @@ struct Engine final : ibpm_handle {
     double *cg_u = nullptr, *cg_r = nullptr, *cg_c = nullptr, *cg_s = nullptr, *cg_s_h = nullptr;
     int *err = nullptr, *err_h = nullptr;
     int last_cg_iters = 0;
-    double last_cg_res = 0.0;
+    double last_cg_res = 0.0, first_cg_res = 0.0, ws_coef[2] = {0.0, 0.0};
     long long launches = 0;
     long long dev_bytes = 0;
     // kernel timing (ibpm_profile)
@@ -213,12 +224,18 @@ struct Engine final : ibpm_handle {
         CK(cudaMemsetAsync(p, 0, n * sizeof(U), st));
         return static_cast<U *>(p);
     }
-    ~Engine() override {
-        if (st) cudaStreamSynchronize(st);
+    // drops the captured step graphs (re-captured on the next step)
+    void drop_graphs() {
         for (int p = 0; p < 2; ++p) {
             if (graph_exec[p]) cudaGraphExecDestroy(graph_exec[p]);
             if (graph[p]) cudaGraphDestroy(graph[p]);
+            graph_exec[p] = nullptr;
+            graph[p] = nullptr;
         }
+    }
+    ~Engine() override {
+        if (st) cudaStreamSynchronize(st);
+        drop_graphs();
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         for (void *p : allocs) cudaFree(p);
         if (prm_h) cudaFreeHost(prm_h);
@@ -461,6 +478,8 @@ struct Engine final : ibpm_handle {
     ibpm_problem problem_copy{};
     T *diag_q = nullptr;
     void set_state(const ibpm_state_view *s) override;
+    void set_warm_start(ibpm_net *net, int mode) override;
+    void warm_start_sample(float *features, float *target, float *prediction) override;
     void get_state(ibpm_state_view *s) override;
     bool advance(int64_t nsteps, const ibpm_step_params *params) override;
     void get_forces(double *fb, double *total) override;
@@ -477,7 +496,7 @@ struct Engine final : ibpm_handle {
     void diag_reg(const double *f, double *gamma1, const double *q1, double *fout) override;
     void setup();
     void build_Binv();
-    void cg(double *x, const double *b);
+    void cg(double *x, const double *b, bool have_bx = false);
     void cg_collect();
     int *cg_it = nullptr;
     bool cg_pending = false, cg_hit_maxiter = false;
@@ -584,7 +603,8 @@ void Engine<T>::setup() {
     // batch width for the B^-1 setup: ~4 GB of column work
     const long long per_col = (2 * ng * L + nq + 2 * ng) * (long long)sizeof(T);
     kbatch = (int)std::max(1LL, std::min<long long>(64, (4LL << 30) / per_col));
-    if (!static_bodies || !std::is_same<T, double>::value) kbatch = 1;  // FP32 builds B^-1 with an FP64 engine
+    if (!std::is_same<T, double>::value) kbatch = 1;  // FP32 builds B^-1 with an FP64 engine
+    if (!static_bodies) kbatch = 2;  // the warm start applies B to two vectors at once
     kbatch = std::min(kbatch, 2 * np);
     const int kb = std::max(kbatch, L);
     t1 = dalloc<T>(ng * kb);
@@ -593,6 +613,21 @@ void Engine<T>::setup() {
     rest = dalloc<T>(ng * L);
     qs1 = dalloc<T>(nq);
     Ftmp = dalloc<double>(2 * np);
+    if (!static_bodies) {
+        Fprev = dalloc<double>(2 * np);
+        ws_z = dalloc<double>(4 * (size_t)np);
+        ws_bz = dalloc<double>(4 * (size_t)np);
+        ws_x2 = dalloc<double>(4 * (size_t)np + 1);  // [x_e | p | |r|]
+        ws_bx2 = dalloc<double>(4 * (size_t)np);
+        ws_feat = dalloc<float>((size_t)kWsFeatures * np);
+        ws_y = dalloc<float>((size_t)kWsOutputs * np);
+        pbody_d = dalloc<int>(np);
+        std::vector<int> pb(np, 0);
+        for (int b = 0; b < nbody; ++b)
+            for (int k = body_start[b]; k < body_start[b + 1]; ++k) pb[k] = b;
+        CK(cudaMemcpyAsync(pbody_d, pb.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
     const int nchunk = (2 * np + 63) / 64;
     part = dalloc<double>((size_t)nchunk * 2 * np);
     patch_stride = 2LL * (nx + 1) * (ny + 1);
@@ -714,6 +749,7 @@ __global__ void cg_init_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h
         a.s[1] = 1.0;
         a.s[2] = tol;
         a.s[3] = cont;
+        a.s[4] = res;  // initial residual, for reports
         a.it[0] = 0;
         if (use_h) cudaGraphSetConditional(h, cont ? 1u : 0u);
     }
@@ -767,10 +803,10 @@ __global__ void cg_update_kernel(CgArgs a, cudaGraphConditionalHandle h, int use
 // capture the loop is a graph WHILE node whose condition the update kernel
 // sets; otherwise the host reads the condition after every iteration.
 template <class T>
-void Engine<T>::cg(double *x, const double *b) {
+void Engine<T>::cg(double *x, const double *b, bool have_bx) {
     const int n = 2 * np;
     CgArgs a{n, x, cg_r, cg_u, cg_c, b, cg_s, cg_it, err, opt.cg_maxiter, opt.cg_reltol, opt.cg_abstol};
-    apply_B(x, cg_c, n, 1);
+    if (!have_bx) apply_B(x, cg_c, n, 1);  // else cg_c already holds B x
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
     if (cs == cudaStreamCaptureStatusActive) {
@@ -831,13 +867,16 @@ void Engine<T>::cg(double *x, const double *b) {
 template <class T>
 void Engine<T>::cg_collect() {
     if (!cg_pending) return;
-    CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_h + 2, cg_it, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_h + 3, err + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     cg_pending = false;
     last_cg_iters = err_h[2];
     last_cg_res = cg_s_h[0];
+    first_cg_res = cg_s_h[4];
+    ws_coef[0] = ws_mode != IBPM_WS_PREVIOUS ? cg_s_h[5] : 0.0;
+    ws_coef[1] = ws_mode == IBPM_WS_LEARNED ? cg_s_h[6] : 0.0;
     if (last_cg_iters >= opt.cg_maxiter) cg_hit_maxiter = true;
     if (err_h[3]) {
         CK(cudaMemsetAsync(err + 2, 0, sizeof(int), st));
@@ -947,7 +986,33 @@ void Engine<T>::step_body() {
         check_launch();
         last_cg_iters = 0;
     } else {
-        cg(Fbt, Ftmp);
+        // CG initial guess.  The reference starts from the previous solution F1
+        // (src/coupling.jl:198-201).  The other modes first take the Galerkin step
+        // in the B-energy norm along the last change d = F1 - F2 (x_e, from B [F1 | d]
+        // in one batched application); the learned mode then maps the residual
+        // b - B x_e to a correction p and takes a second Galerkin step along p.
+        launch_ws_direction(Fbt, Fprev, np, ws_z, st);
+        check_launch();
+        if (ws_mode == IBPM_WS_PREVIOUS) {
+            cg(Fbt, Ftmp);
+        } else {
+            apply_B(ws_z, ws_bz, 2 * np, 2);
+            launch_ws_galerkin(ws_z, ws_bz, Ftmp, Fbt, cg_c, ws_x2, ws_bx2, np, 1, cg_s + 5, st);
+            check_launch();
+            launch_ws_features(Ftmp, cg_c, ws_z, ws_z + 2 * np, P.ub, motion, pbody_d, np, ws_feat, ws_x2 + 4 * np,
+                               st);
+            check_launch();
+            if (ws_mode == IBPM_WS_LEARNED) {
+                net_forward_dev(ws, ws_feat, 1, np, ws_act, ws_y, st);
+                check_launch();
+                launch_ws_prediction(ws_y, ws, np, ws_x2 + 2 * np, st);
+                check_launch();
+                apply_B(ws_x2 + 2 * np, ws_bx2 + 2 * np, 2 * np, 1);
+                launch_ws_galerkin(ws_x2, ws_bx2, Ftmp, Fbt, cg_c, nullptr, nullptr, np, 1, cg_s + 6, st);
+                check_launch();
+            }
+            cg(Fbt, Ftmp, true);
+        }
         cg_pending = true;
         binv_reduce_kernel<<<1, 1024, 0, st>>>(nullptr, 0, n, Fbt, fb, total, g.h, g.dt, 0);
         check_launch();
@@ -1067,6 +1132,57 @@ void Engine<T>::init(const ibpm_problem *p, const ibpm_options &o) {
 }
 
 template <class T>
+void Engine<T>::set_warm_start(ibpm_net *net, int mode) {
+    CK(cudaSetDevice(device));
+    if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
+    if (mode != IBPM_WS_PREVIOUS && mode != IBPM_WS_LEARNED && mode != IBPM_WS_EXTRAPOLATED)
+        throw ApiError{IBPM_ERR_INVALID, "unknown warm-start mode"};
+    if (mode == IBPM_WS_LEARNED && !net) throw ApiError{IBPM_ERR_INVALID, "the learned warm start needs a network"};
+    if (mode != IBPM_WS_LEARNED) net = nullptr;
+    if (net) {
+        if (net_device(net) != device) throw ApiError{IBPM_ERR_INVALID, "network and solver are on different devices"};
+        if (net_cin(net) != kWsFeatures || net_cout(net) != kWsOutputs)
+            throw ApiError{IBPM_ERR_INVALID, "the warm-start network must map 10 feature channels to 2 outputs"};
+        const size_t need = net_act_floats(net, 1, np);
+        if (need > ws_act_cap) {
+            ws_act = dalloc<float>(need);
+            ws_act_cap = need;
+        }
+    }
+    CK(cudaStreamSynchronize(st));
+    ws = net;
+    ws_mode = mode;
+    drop_graphs();  // the step graph holds the previous choice
+}
+
+template <class T>
+void Engine<T>::warm_start_sample(float *features, float *target, float *prediction) {
+    CK(cudaSetDevice(device));
+    if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
+    if (ws_mode == IBPM_WS_PREVIOUS)
+        throw ApiError{IBPM_ERR_INVALID, "warm-start samples need the extrapolated or learned mode"};
+    std::vector<double> f(2 * np), xe(2 * np);
+    double rs = 0.0;
+    CK(cudaMemcpyAsync(f.data(), Fbt, sizeof(double) * 2 * np, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(xe.data(), ws_x2, sizeof(double) * 2 * np, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&rs, ws_x2 + 4 * np, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (features)
+        CK(cudaMemcpyAsync(features, ws_feat, sizeof(float) * kWsFeatures * np, cudaMemcpyDeviceToHost, st));
+    std::vector<double> pv(2 * np, 0.0);
+    if (prediction && ws_mode == IBPM_WS_LEARNED)
+        CK(cudaMemcpyAsync(pv.data(), ws_x2 + 2 * np, sizeof(double) * 2 * np, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // the error of the extrapolated guess, converged F~b - x_e, in units of the
+    // RMS of its residual (the scale of the residual feature channels)
+    const double inv = rs > 0.0 ? 1.0 / rs : 0.0;
+    if (target)
+        for (int i = 0; i < 2 * np; ++i) target[i] = (float)((f[i] - xe[i]) * inv);
+    // the network's correction as the step used it
+    if (prediction)
+        for (int i = 0; i < 2 * np; ++i) prediction[i] = (float)pv[i];
+}
+
+template <class T>
 void Engine<T>::set_state(const ibpm_state_view *s) {
     CK(cudaSetDevice(device));
     const size_t ngL = (size_t)(ng * L), nqL = (size_t)(nq * L);
@@ -1087,6 +1203,7 @@ void Engine<T>::set_state(const ibpm_state_view *s) {
     if (s->ds) CK(cudaMemcpyAsync(ds, s->ds, np2 / 2, cudaMemcpyHostToDevice, st));
     if (s->ub) CK(cudaMemcpyAsync(P.ub, s->ub, np2, cudaMemcpyHostToDevice, st));
     if (s->fbt) CK(cudaMemcpyAsync(Fbt, s->fbt, np2, cudaMemcpyHostToDevice, st));
+    if (s->fbt && Fprev) CK(cudaMemcpyAsync(Fprev, Fbt, np2, cudaMemcpyDeviceToDevice, st));
     fs_last[0] = s->freestream[0];
     fs_last[1] = s->freestream[1];
     // update_vars! (problem.jl:676-685)
@@ -1152,6 +1269,9 @@ void Engine<T>::get_info(ibpm_info *info) {
     info->static_bodies = static_bodies ? 1 : 0;
     info->last_cg_iters = last_cg_iters;
     info->last_cg_residual = last_cg_res;
+    info->first_cg_residual = first_cg_res;
+    info->warm_start_coef[0] = ws_coef[0];
+    info->warm_start_coef[1] = ws_coef[1];
     info->device_bytes = dev_bytes;
 }
 
@@ -1348,6 +1468,16 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
 }
 
 void ibpm_destroy(ibpm_handle *h) { delete h; }
+
+int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net) {
+    if (!h) return IBPM_ERR_INVALID;
+    return guarded(h, [&] { h->set_warm_start(net, mode); });
+}
+
+int ibpm_warm_start_sample(ibpm_handle *h, float *features, float *target, float *prediction) {
+    if (!h) return IBPM_ERR_INVALID;
+    return guarded(h, [&] { h->warm_start_sample(features, target, prediction); });
+}
 
 int ibpm_set_state(ibpm_handle *h, const ibpm_state_view *s) {
     if (!h || !s) return IBPM_ERR_INVALID;

@@ -212,6 +212,29 @@ class GpuCnabSolver(AbstractSolver):
         _abi.check(self.lib, self._h, self.lib.ibpm_diag_reg(self._h, None, None, _abi.dptr(q1), _abi.dptr(out)))
         return out
 
+    def set_warm_start(self, net=None, mode: Optional[str] = None):
+        """CG initial guess of this moving-body solver: "previous" (the reference's
+        start from the previous F~b), "learned" (along a `WarmStartNet`'s predicted
+        change; the default when net is given) or "extrapolated" (along the last
+        change F1 - F2).  Keep the network alive while it is installed."""
+        mode = mode or ("learned" if net is not None else "previous")
+        m = {"previous": _abi.IBPM_WS_PREVIOUS, "learned": _abi.IBPM_WS_LEARNED,
+             "extrapolated": _abi.IBPM_WS_EXTRAPOLATED}[mode]
+        _abi.check(self.lib, self._h, self.lib.ibpm_set_warm_start(self._h, m, net.handle if net is not None else None))
+        self._warm_net = net
+
+    def warm_start_sample(self, prediction: bool = False):
+        """(features [10][np], target [2][np]) of the last step: the warm start's
+        inputs and the error of its extrapolated guess (converged F~b - x_e); with
+        prediction=True also the network's correction as the step used it."""
+        n = self.state.prob.bodies.npanel
+        f = np.empty((10, n), dtype=np.float32)
+        t = np.empty((2, n), dtype=np.float32)
+        p = np.empty((2, n), dtype=np.float32) if prediction else None
+        _abi.check(self.lib, self._h, self.lib.ibpm_warm_start_sample(self._h, _abi.fptr(f), _abi.fptr(t),
+                                                                       _abi.fptr(p)))
+        return (f, t, p) if prediction else (f, t)
+
     def advance_many(self, nsteps: int):
         """nsteps advance! calls in one library call (params evaluated on the host
         up front); the host State's index/t/fb are updated at the end."""

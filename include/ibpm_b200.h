@@ -106,6 +106,9 @@ typedef struct ibpm_info {
     int32_t last_cg_iters;      /* iterations of the last step's CG (0 for static bodies) */
     double last_cg_residual;    /* final ||r|| of that CG */
     int64_t device_bytes;       /* device memory held by the handle */
+    double first_cg_residual;   /* ||r0|| of the last step's CG, from its initial guess */
+    double warm_start_coef[2];  /* the last step's warm-start Galerkin coefficients: along
+                                   F1 - F2, then along the network's correction */
 } ibpm_info;
 
 typedef struct ibpm_handle ibpm_handle;
@@ -173,6 +176,70 @@ int ibpm_diag_vort2flux(ibpm_handle *h, double *gamma, double *psi, double *q);
 /* rot!(reg!(f)) (fluid.jl:101-111 after coupling.jl:72-85) into gamma1 (ng), and
  * regT!(f, q1) (coupling.jl:57-69) from a level-1 flux q1 (nq); NULL skips either. */
 int ibpm_diag_reg(ibpm_handle *h, const double *f, double *gamma1, const double *q1, double *fout);
+
+/* Learned CG warm start for moving bodies.  No counterpart in the reference:
+ * cg! (src/coupling.jl:194-202) starts from the previous F~b.  Here the start
+ * can first move along the last change of the solution (a Galerkin step in the
+ * B-energy norm), and then along a network's correction computed from that
+ * guess's residual; plain CG then runs to the same tolerance, so only the
+ * iteration count changes.
+ *
+ * The network is a 1D convolutional net over the body points: `layers`
+ * convolutions of odd width `kernel` with zero padding, `width` channels
+ * between them, tanh after every layer but the last.  Inputs are normalised per
+ * channel ((x - in_mean) / in_std) and the last layer's output is the
+ * normalised prediction (prediction = out_mean + out_std * y).  Parameters are
+ * one FP32 vector: per layer W [out][in][kernel], then b [out].  Samples are
+ * arrays [batch][channels][n], n body points per sample.  The warm start uses
+ * 10 input channels per point -- the residual r = b - B x_e of the
+ * extrapolated guess x_e (x, y), the previous solution F1 (x, y), its last
+ * change d = F1 - F2 (x, y), ub (x, y), cos and sin of the body angle, with r and
+ * d divided by their RMS over the sample -- and 2 outputs, the correction of x_e
+ * (x, y) in units of r's RMS.  A network lives on one device and owns a stream. */
+typedef struct ibpm_net ibpm_net;
+int ibpm_net_create(int32_t cin, int32_t width, int32_t kernel, int32_t layers, int32_t cout, uint64_t seed,
+                    int32_t device, ibpm_net **out);
+void ibpm_net_destroy(ibpm_net *net);
+int64_t ibpm_net_num_params(const ibpm_net *net);
+int ibpm_net_get_params(ibpm_net *net, float *params);
+int ibpm_net_set_params(ibpm_net *net, const float *params);   /* also resets the optimiser state */
+int ibpm_net_set_normalisation(ibpm_net *net, const float *in_mean, const float *in_std, const float *out_mean,
+                               const float *out_std);
+int ibpm_net_get_normalisation(ibpm_net *net, float *in_mean, float *in_std, float *out_mean, float *out_std);
+/* Prediction in solver units for raw host samples x [batch][cin][n] -> y [batch][cout][n]. */
+int ibpm_net_forward(ibpm_net *net, const float *x, int64_t batch, int32_t n, float *y);
+/* Loss of the normalised prediction against the normalised raw targets
+ * t [batch][cout][n], and its gradient with respect to the parameters.  With e
+ * the error of one sequence of n points and E its running sum along the points
+ * divided by sqrt(n), the loss is (sum e^2 + sum E^2) / (batch cout n): the
+ * running-sum term weighs the smooth error components, the ones that dominate
+ * the CG residual, about n/3 times more. */
+int ibpm_net_loss_grad(ibpm_net *net, const float *x, const float *t, int64_t batch, int32_t n, float *loss,
+                       float *grad);
+/* Adam (lr, betas 0.9 / 0.999, eps 1e-8) on shuffled full batches of the raw
+ * samples, `epochs` passes; epoch_loss[e] (may be NULL) is the mean batch loss. */
+int ibpm_net_train(ibpm_net *net, const float *x, const float *t, int64_t nsamples, int32_t n, int32_t epochs,
+                   int32_t batch, float lr, uint64_t seed, float *epoch_loss);
+const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed create */
+/* Chooses the CG initial guess of a moving-body handle.  F1, F2 are the last two
+ * solutions:
+ *   IBPM_WS_PREVIOUS      F1 (the reference; net ignored)
+ *   IBPM_WS_EXTRAPOLATED  x_e = F1 + y (F1 - F2)
+ *   IBPM_WS_LEARNED       x_e + a p, p the network's correction from x_e's residual
+ *                         (net: 10 -> 2 channels on the handle's device, kept alive
+ *                         while installed)
+ * where y and a minimise the B-energy norm of the error along their directions
+ * (Galerkin steps; B is applied to [F1 | F1 - F2] in one batched pass and once
+ * more to p; CG reuses B x0). */
+#define IBPM_WS_PREVIOUS 0
+#define IBPM_WS_LEARNED 1
+#define IBPM_WS_EXTRAPOLATED 2
+int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net);
+/* The last step's warm-start features (10 x npanel floats), target (2 x
+ * npanel: the converged F~b minus the extrapolated guess x_e) and, in the
+ * learned mode, the network's correction as the step used it (zeros
+ * otherwise); the target is in units of the RMS of x_e's residual.  Needs the extrapolated or learned mode; NULL skips an output. */
+int ibpm_warm_start_sample(ibpm_handle *h, float *features, float *target, float *prediction);
 
 /* Laplacian-inverse solve x = Δ⁻¹ b (the operator of src/fluid.jl:117-119) for callers
  * that cannot allocate device memory.  No counterpart in the reference: it exists
