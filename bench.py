@@ -230,6 +230,41 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
             "steps_per_s_vs_previous": {m: out[m]["steps_per_s"] / base["steps_per_s"] for m in out}}
 
 
+def ensemble_report(ib, device: int, seed: int = 2026, n: int = 128, steps: int = 10):
+    """Case-steps/s of n independent FP32 cases (finest grids of {256, 384, 512} x
+    256 cells at h 0.01, 3 levels, seeded cylinders or plates, Re ~ U[50, 300],
+    dt 0.002) stepped together (ibpm_ensemble_advance), against the same cases
+    stepped one after another.  Host-timed between device synchronisations (the
+    cases run on n streams)."""
+    import torch
+
+    probs = ib.configs.ensemble_cases(n, seed=seed)
+    t0 = time.perf_counter()
+    solvers = [ib.GpuCnabSolver(ib.State(p), precision="fp32", device=device) for p in probs]
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    ens = ib.Ensemble(solvers)
+    ens.advance_(3, fetch_forces=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens.advance_(steps, fetch_forces=False)
+    torch.cuda.synchronize()
+    t_conc = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for s in solvers:
+        s.advance_many(steps)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    pts = sum(p.grid.base.n[0] * p.grid.base.n[1] * p.grid.nlevel for p in probs)
+    forces = ens.total_forces()
+    return {"workload": f"{n} seeded cases (seed {seed}): {{256, 384, 512}} x 256 cells at h 0.01, 3 levels, "
+                        "cylinders D ~ U[0.5, 1.5] or plates at AoA ~ U[0, 45] deg, Re ~ U[50, 300], dt 0.002, FP32",
+            "setup_s": t_setup, "steps": steps, "case_steps_per_s": n * steps / t_conc,
+            "grid_point_updates_per_s": pts * steps / t_conc, "ms_per_ensemble_step": 1000.0 * t_conc / steps,
+            "sequential_case_steps_per_s": n * steps / t_seq, "speedup_vs_sequential": t_seq / t_conc,
+            "forces_finite": bool(np.isfinite(forces).all()), "timing": "host clock between device synchronisations"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -259,6 +294,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-chosen", action="store_true", help="skip the mixed-precision engine")
     ap.add_argument("--no-learned", action="store_true", help="skip the moving-body CG warm-start comparison")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 128-case ensemble measurement")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
@@ -386,6 +422,7 @@ def main():
                   "meets_bar": bool(dC <= 1e-4 and vort <= 1e-5)}
 
     learned = None if args.no_learned else warm_start_report(ib, local)
+    ensemble = None if args.no_ensemble else ensemble_report(ib, local, seed=2026 + rank)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -411,7 +448,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps, "api": "GpuCnabSolver.advance_ (ctypes -> ibpm_advance + ibpm_get_forces)"},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-                "chosen_form": chosen, "learned_warm_start": learned}
+                "chosen_form": chosen, "learned_warm_start": learned, "ensemble": ensemble}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

@@ -6,6 +6,7 @@ synthetic and seeded (no dataset is involved):
   cylinder_re100_1024     1024 x 1024, 5 levels, 628 points, Re 100, dt 0.001, Γ noise 1e-3 (seed 12345)
   plate_aoa30_1024        1024 x 1024, 5 levels, 201-point flat plate at 30 deg, Re 200, dt 0.001
   pitching_plate_512      512 x 512, 4 levels, 101-point plate pitching/plunging, Re 500, dt 0.002
+  ensemble_cases          seeded cases of {256, 384, 512} x 256 cells, 3 levels, cylinders or plates (seed 2026)
   small_cylinder          a few-second case for tests (any size)
 """
 from __future__ import annotations
@@ -83,3 +84,32 @@ def small_cylinder(n=64, nlevel=3, npts=None, Re=100.0, dt=None) -> Problem:
     h = 4.0 / n
     npts = npts or max(16, int(round(math.pi / h)))
     return cylinder(h, (-1.0, 3.0), (-2.0, 2.0), nlevel, npts, Re, dt or 0.2 * h)
+
+
+def ensemble_cases(n: int = 128, seed: int = 2026, h: float = 0.01, nlevel: int = 3, dt: float = 0.002,
+                   widths=(256, 384, 512), ny: int = 256):
+    """n independent cases from a seeded generator: a finest grid of nx x ny
+    cells (nx drawn from `widths`) at spacing h with `nlevel` levels; a static
+    cylinder of diameter D ~ U[0.5, 1.5] or a flat plate of chord 1 at an angle
+    of attack ~ U[0, 45] deg, with body points about h apart; Re ~ U[50, 300];
+    uniform flow (1, 0).  Returns the list of Problems."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx = int(rng.choice(widths))
+        Re = float(rng.uniform(50.0, 300.0))
+        W, H = nx * h, ny * h
+        xlims, ylims = (-0.4 * H, -0.4 * H + W), (-0.5 * H, 0.5 * H)
+        fluid = Fluid(grid=fluid_grid(h=h, xlims=xlims, ylims=ylims, nlevel=nlevel), Re=Re,
+                      freestream_vel=uniform_flow)
+        if rng.uniform() < 0.5:
+            D = float(rng.uniform(0.5, 1.5))
+            panels = Curves.partition(Curves.Circle(r=D / 2, center=(0.0, 0.0)), int(round(math.pi * D / h)))
+            body = Bodies(cyl=StaticBody(panels))
+        else:
+            aoa = math.radians(float(rng.uniform(0.0, 45.0)))
+            c, s = 0.5 * math.cos(aoa), 0.5 * math.sin(aoa)
+            panels = Curves.partition(Curves.LineSegment((-c, s), (c, -s)), int(round(1.0 / h)))
+            body = Bodies(plate=StaticBody(panels))
+        out.append(Problem(fluid=fluid, bodies=body, scheme=CNAB(dt=dt)))
+    return out

@@ -108,6 +108,10 @@ struct ibpm_handle {
     virtual void set_state(const ibpm_state_view *s) = 0;
     virtual void get_state(ibpm_state_view *s) = 0;
     virtual bool advance(int64_t nsteps, const ibpm_step_params *params) = 0;  // true: CG hit maxiter
+    // one step enqueued on the handle's stream without waiting for it (ensembles)
+    virtual void enqueue_step(const ibpm_step_params &prm) = 0;
+    // waits for the enqueued steps; true: a CG hit maxiter
+    virtual bool finish_steps() = 0;
     virtual void get_forces(double *fb, double *total) = 0;
     virtual void get_time(int64_t *index, double *t) = 0;
     virtual void get_info(ibpm_info *info) = 0;
@@ -158,6 +162,26 @@ struct Engine final : ibpm_handle {
     double *Fbt = nullptr, *fb = nullptr, *total = nullptr;
     StepDev *prm = nullptr, *prm_h = nullptr;
     double *motion = nullptr, *motion_h = nullptr;
+    // Pinned staging of the per-step parameters: a ring of slots, each reused only
+    // after the copies that read it have run (asynchronous copies read pinned
+    // host memory when they execute, not when they are enqueued).
+    static constexpr int kStage = 8;
+    StepDev *stage_prm[kStage] = {};
+    double *stage_motion[kStage] = {};
+    cudaEvent_t stage_ev[kStage] = {};
+    bool stage_used[kStage] = {};
+    int stage_next = 0;
+    // next free slot: prm_h / motion_h point into it
+    void stage_acquire() {
+        const int k = stage_next;
+        stage_next = (stage_next + 1) % kStage;
+        if (stage_used[k]) CK(cudaEventSynchronize(stage_ev[k]));
+        prm_h = stage_prm[k];
+        motion_h = stage_motion[k];
+        stage_used[k] = true;
+    }
+    // marks the slot just used as busy until the stream reaches this point
+    void stage_release() { CK(cudaEventRecord(stage_ev[(stage_next + kStage - 1) % kStage], st)); }
     // learned CG warm start (moving bodies): the installed network, the solution
     // of two steps back, the features and prediction of the current step
     ibpm_net *ws = nullptr;
@@ -212,6 +236,36 @@ struct Engine final : ibpm_handle {
         prof_recs.push_back(ProfRec{cls, i, bytes});
     }
     std::vector<void *> allocs;
+    std::vector<long long> alloc_bytes;  // size of each entry of allocs
+    // frees one allocation of this handle
+    void dfree(void *p) {
+        if (!p) return;
+        auto it = std::find(allocs.begin(), allocs.end(), p);
+        if (it != allocs.end()) {
+            const size_t i = (size_t)(it - allocs.begin());
+            dev_bytes -= alloc_bytes[i];
+            alloc_bytes.erase(alloc_bytes.begin() + (long)i);
+            allocs.erase(it);
+        }
+        cudaFree(p);
+    }
+    // After the B^-1 setup a static-body handle applies B to one vector at a time:
+    // the setup's column-batch buffers shrink to one column.
+    void shrink_batch_buffers() {
+        if (kbatch <= 1) return;
+        CK(cudaStreamSynchronize(st));
+        for (void *p : {(void *)t1, (void *)t2, (void *)patch, (void *)Gw, (void *)psiw, (void *)qw, (void *)fcol})
+            dfree(p);
+        kbatch = 1;
+        const int kb = std::max(1, L);
+        t1 = dalloc<T>(ng * kb);
+        t2 = dalloc<T>(ng * kb);
+        patch = dalloc<T>(patch_stride);
+        Gw = dalloc<T>(ng * L);
+        psiw = dalloc<T>(ng * L);
+        qw = dalloc<T>(nq);
+        fcol = dalloc<double>(2 * (size_t)np);
+    }
 
     template <class U>
     U *dalloc(size_t n) {
@@ -220,6 +274,7 @@ struct Engine final : ibpm_handle {
         cudaError_t e = cudaMalloc(&p, n * sizeof(U));
         if (e != cudaSuccess) throw ApiError{IBPM_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(U)) + " bytes failed"};
         allocs.push_back(p);
+        alloc_bytes.push_back((long long)(n * sizeof(U)));
         dev_bytes += (long long)(n * sizeof(U));
         CK(cudaMemsetAsync(p, 0, n * sizeof(U), st));
         return static_cast<U *>(p);
@@ -238,8 +293,11 @@ struct Engine final : ibpm_handle {
         drop_graphs();
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         for (void *p : allocs) cudaFree(p);
-        if (prm_h) cudaFreeHost(prm_h);
-        if (motion_h) cudaFreeHost(motion_h);
+        for (int k = 0; k < kStage; ++k) {
+            if (stage_prm[k]) cudaFreeHost(stage_prm[k]);
+            if (stage_motion[k]) cudaFreeHost(stage_motion[k]);
+            if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
+        }
         if (cg_s_h) cudaFreeHost(cg_s_h);
         if (err_h) cudaFreeHost(err_h);
         if (st_side) cudaStreamDestroy(st_side);
@@ -482,6 +540,18 @@ struct Engine final : ibpm_handle {
     void warm_start_sample(float *features, float *target, float *prediction) override;
     void get_state(ibpm_state_view *s) override;
     bool advance(int64_t nsteps, const ibpm_step_params *params) override;
+    void enqueue_step(const ibpm_step_params &prm) override {
+        CK(cudaSetDevice(device));
+        step(prm);
+    }
+    bool finish_steps() override {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamSynchronize(st));
+        cg_collect();
+        const bool m = cg_hit_maxiter;
+        cg_hit_maxiter = false;
+        return m;
+    }
     void get_forces(double *fb, double *total) override;
     void get_time(int64_t *index, double *t) override;
     void get_info(ibpm_info *info) override;
@@ -593,8 +663,14 @@ void Engine<T>::setup() {
     total = dalloc<double>(2);
     prm = dalloc<StepDev>(1);
     motion = dalloc<double>(6 * (size_t)std::max(nbody, 1));
-    CK(cudaMallocHost(&prm_h, sizeof(StepDev)));
-    CK(cudaMallocHost(&motion_h, sizeof(double) * 6 * std::max(nbody, 1)));
+    for (int k = 0; k < kStage; ++k) {
+        CK(cudaMallocHost(&stage_prm[k], sizeof(StepDev)));
+        CK(cudaMallocHost(&stage_motion[k], sizeof(double) * 6 * std::max(nbody, 1)));
+        CK(cudaEventCreateWithFlags(&stage_ev[k], cudaEventDisableTiming));
+        memset(stage_prm[k], 0, sizeof(StepDev));
+    }
+    prm_h = stage_prm[0];
+    motion_h = stage_motion[0];
     CK(cudaMallocHost(&cg_s_h, sizeof(double) * 8));
     CK(cudaMallocHost(&err_h, sizeof(int) * 4));
     memset(prm_h, 0, sizeof(StepDev));
@@ -661,6 +737,7 @@ void Engine<T>::setup() {
         compute_bbox();
         if (std::is_same<T, double>::value) {
             build_Binv();
+            shrink_batch_buffers();
         } else {
             // B and B^-1 in FP64 with a temporary FP64 engine of the same problem;
             // only the (2np)^2 matrix is kept.
@@ -889,6 +966,7 @@ template <class T>
 void Engine<T>::step(const ibpm_step_params &sp) {
     // inc_time_index! and the host callbacks' values
     ++index;
+    stage_acquire();
     prm_h->fs[0] = sp.freestream[0];
     prm_h->fs[1] = sp.freestream[1];
     for (int k = 0; k < 6; ++k) prm_h->gm[k] = sp.grid_motion[k];
@@ -911,6 +989,7 @@ void Engine<T>::step(const ibpm_step_params &sp) {
         compute_bbox();
         check_region_error();
     }
+    stage_release();
     q0_zero = false;
     q0_from_user = false;
     // The rest of the step is one CUDA graph per parity of the ping-ponged
@@ -1091,10 +1170,12 @@ void Engine<T>::materialise_q0() {
         CK(cudaMemsetAsync(q0mat, 0, sizeof(T) * nq * L, st));
         return;
     }
+    stage_acquire();
     prm_h->fs[0] = fs_last[0];
     prm_h->fs[1] = fs_last[1];
     for (int k = 0; k < 6; ++k) prm_h->gm[k] = gm_last[k];
     CK(cudaMemcpyAsync(prm, prm_h, sizeof(StepDev), cudaMemcpyHostToDevice, st));
+    stage_release();
     q0_fill_kernel<T><<<dim3((unsigned)((nq + 255) / 256), L), 256, 0, st>>>(q0mat, prm, g);
     check_launch();
 }
@@ -1500,6 +1581,61 @@ int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params)
     }
     return IBPM_OK;
 }
+
+struct ibpm_ensemble {
+    std::vector<ibpm_handle *> cases;
+    std::string last_error;
+};
+
+int ibpm_ensemble_create(ibpm_handle *const *cases, int32_t n, ibpm_ensemble **out) {
+    if (!out) return IBPM_ERR_INVALID;
+    *out = nullptr;
+    if (n < 1 || !cases) return IBPM_ERR_INVALID;
+    for (int32_t c = 0; c < n; ++c)
+        if (!cases[c]) return IBPM_ERR_INVALID;
+    ibpm_ensemble *e = new ibpm_ensemble;
+    e->cases.assign(cases, cases + n);
+    *out = e;
+    return IBPM_OK;
+}
+
+void ibpm_ensemble_destroy(ibpm_ensemble *e) { delete e; }
+
+// Round-robin over the cases: each step of every case is enqueued on that case's
+// own stream before any is waited for, so the cases' step graphs run side by
+// side on the GPU.
+int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_params *params) {
+    if (!e || nsteps < 0 || (nsteps > 0 && !params)) return IBPM_ERR_INVALID;
+    const int64_t n = (int64_t)e->cases.size();
+    for (int64_t k = 0; k < nsteps; ++k)
+        for (int64_t c = 0; c < n; ++c) {
+            ibpm_handle *h = e->cases[c];
+            const int rc = guarded(h, [&] { h->enqueue_step(params[k * n + c]); });
+            if (rc != IBPM_OK) {
+                e->last_error = "case " + std::to_string(c) + ": " + h->last_error;
+                for (ibpm_handle *o : e->cases) guarded(o, [&] { o->finish_steps(); });
+                return rc;
+            }
+        }
+    bool maxiter = false;
+    for (int64_t c = 0; c < n; ++c) {
+        ibpm_handle *h = e->cases[c];
+        bool m = false;
+        const int rc = guarded(h, [&] { m = h->finish_steps(); });
+        if (rc != IBPM_OK) {
+            e->last_error = "case " + std::to_string(c) + ": " + h->last_error;
+            return rc;
+        }
+        maxiter = maxiter || m;
+    }
+    if (maxiter) {
+        e->last_error = "CG reached maxiter";
+        return IBPM_WARN_CG_MAXITER;
+    }
+    return IBPM_OK;
+}
+
+const char *ibpm_ensemble_last_error(const ibpm_ensemble *e) { return e ? e->last_error.c_str() : ""; }
 
 int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force) {
     if (!h) return IBPM_ERR_INVALID;

@@ -136,6 +136,19 @@ int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params)
 /* state.fb (npanel x 2) and boundary_total_force over all panels (2); NULL skips. */
 int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force);
 
+/* Ensembles: independent cases (handles of any sizes, bodies and precisions)
+ * stepped together.  No counterpart in the reference, which steps one case per
+ * solver.  ibpm_ensemble_advance enqueues every case's step on that case's own
+ * stream before waiting for any, so the cases' step graphs run side by side;
+ * params[k * n + c] holds step k of case c.  Each case's results are those of
+ * stepping it alone.  Static-body cases overlap fully; a moving-body case waits
+ * for its region check every step.  The ensemble does not own the handles. */
+typedef struct ibpm_ensemble ibpm_ensemble;
+int ibpm_ensemble_create(ibpm_handle *const *cases, int32_t n, ibpm_ensemble **out);
+int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_params *params);
+void ibpm_ensemble_destroy(ibpm_ensemble *e);
+const char *ibpm_ensemble_last_error(const ibpm_ensemble *e);
+
 int ibpm_get_time(ibpm_handle *h, int64_t *index, double *t);
 int ibpm_get_info(ibpm_handle *h, ibpm_info *info);
 const char *ibpm_last_error(const ibpm_handle *h);
