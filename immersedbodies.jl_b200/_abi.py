@@ -67,6 +67,7 @@ EXPORTS = {
     "ibpm_get_state": (C.c_int, [C.c_void_p, C.POINTER(ibpm_state_view)]),
     "ibpm_advance": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(ibpm_step_params)]),
     "ibpm_get_forces": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "ibpm_get_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "ibpm_get_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), _dp]),
     "ibpm_get_info": (C.c_int, [C.c_void_p, C.POINTER(ibpm_info)]),
     "ibpm_last_error": (C.c_char_p, [C.c_void_p]),

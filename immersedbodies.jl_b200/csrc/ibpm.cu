@@ -107,6 +107,7 @@ struct ibpm_handle {
     virtual ~ibpm_handle() {}
     virtual void set_state(const ibpm_state_view *s) = 0;
     virtual void get_state(ibpm_state_view *s) = 0;
+    virtual void get_field(int field, int level, double *out) = 0;
     virtual bool advance(int64_t nsteps, const ibpm_step_params *params) = 0;  // true: CG hit maxiter
     // one step enqueued on the handle's stream without waiting for it (ensembles)
     virtual void enqueue_step(const ibpm_step_params &prm) = 0;
@@ -536,7 +537,9 @@ struct Engine final : ibpm_handle {
     ibpm_problem problem_copy{};
     T *diag_q = nullptr;
     void set_state(const ibpm_state_view *s) override;
-    void set_warm_start(ibpm_net *net, int mode) override;
+    void get_field(int field, int level, double *out) override;
+    double *field_d = nullptr;  // one level of an output field
+        void set_warm_start(ibpm_net *net, int mode) override;
     void warm_start_sample(float *features, float *target, float *prediction) override;
     void get_state(ibpm_state_view *s) override;
     bool advance(int64_t nsteps, const ibpm_step_params *params) override;
@@ -1212,6 +1215,49 @@ void Engine<T>::init(const ibpm_problem *p, const ibpm_options &o) {
     problem_copy.body_ds = ref_ds.data();
 }
 
+namespace {
+// Output accessors (src/problem.jl:715-866) for one level: vorticity Gamma / hc^2,
+// x_velocity (q_u + q0_u) / hc, y_velocity (q_v + q0_v) / hc.
+template <class T>
+__global__ void field_kernel(const T *__restrict__ G, const T *__restrict__ q, const T *__restrict__ q0, int field,
+                             int lev, Grid g, double *__restrict__ out) {
+    const long long nu = (long long)(g.nx + 1) * g.ny, nq = nu + (long long)g.nx * (g.ny + 1);
+    const long long ng = (long long)(g.nx - 1) * (g.ny - 1);
+    const long long n = field == IBPM_FIELD_VORTICITY ? ng : field == IBPM_FIELD_X_VELOCITY ? nu : nq - nu;
+    const double hc = gridstep(g, lev);
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        if (field == IBPM_FIELD_VORTICITY) {
+            out[k] = (double)G[(lev - 1) * ng + k] / (hc * hc);
+        } else {
+            const long long f = (lev - 1) * nq + (field == IBPM_FIELD_X_VELOCITY ? k : nu + k);
+            out[k] = ((double)q[f] + (double)q0[f]) / hc;
+        }
+    }
+}
+}  // namespace
+
+template <class T>
+void Engine<T>::get_field(int field, int level, double *out) {
+    CK(cudaSetDevice(device));
+    if (level < 1 || level > L) throw ApiError{IBPM_ERR_INVALID, "level out of range"};
+    long long n = 0;
+    if (field == IBPM_FIELD_VORTICITY)
+        n = ng;
+    else if (field == IBPM_FIELD_X_VELOCITY)
+        n = (long long)(nx + 1) * ny;
+    else if (field == IBPM_FIELD_Y_VELOCITY)
+        n = (long long)nx * (ny + 1);
+    else
+        throw ApiError{IBPM_ERR_INVALID, "unknown field"};
+    if (!out) throw ApiError{IBPM_ERR_INVALID, "null output"};
+    if (!field_d) field_d = dalloc<double>((size_t)std::max<long long>(nq, ng));
+    if (field != IBPM_FIELD_VORTICITY) materialise_q0();
+    field_kernel<T><<<592, 256, 0, st>>>(G[gc], q, q0mat, field, level, g, field_d);
+    check_launch();
+    CK(cudaMemcpyAsync(out, field_d, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+}
+
 template <class T>
 void Engine<T>::set_warm_start(ibpm_net *net, int mode) {
     CK(cudaSetDevice(device));
@@ -1636,6 +1682,11 @@ int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_para
 }
 
 const char *ibpm_ensemble_last_error(const ibpm_ensemble *e) { return e ? e->last_error.c_str() : ""; }
+
+int ibpm_get_field(ibpm_handle *h, int32_t field, int32_t level, double *out) {
+    if (!h) return IBPM_ERR_INVALID;
+    return guarded(h, [&] { h->get_field(field, level, out); });
+}
 
 int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force) {
     if (!h) return IBPM_ERR_INVALID;

@@ -145,6 +145,26 @@ class GpuCnabSolver(AbstractSolver):
         _abi.check(self.lib, self._h, self.lib.ibpm_get_forces(self._h, _abi.dptr(s.fb), None))
         self._stale = True
 
+    def _field(self, field: int, level: int, shape) -> np.ndarray:
+        out = np.empty(shape, order="F")
+        _abi.check(self.lib, self._h, self.lib.ibpm_get_field(self._h, field, level, _abi.dptr(out)))
+        return out
+
+    def vorticity(self, level: int = 1) -> np.ndarray:
+        """vorticity! of one level (1-based), computed on the device: Γ / hc², (nx-1) x (ny-1)."""
+        nx, ny = self.state.prob.grid.base.n
+        return self._field(0, level, (nx - 1, ny - 1))
+
+    def x_velocity(self, level: int = 1) -> np.ndarray:
+        """x_velocity! of one level, computed on the device: (q + q0)_u / hc, (nx+1) x ny."""
+        nx, ny = self.state.prob.grid.base.n
+        return self._field(1, level, (nx + 1, ny))
+
+    def y_velocity(self, level: int = 1) -> np.ndarray:
+        """y_velocity! of one level, computed on the device: (q + q0)_v / hc, nx x (ny+1)."""
+        nx, ny = self.state.prob.grid.base.n
+        return self._field(2, level, (nx, ny + 1))
+
     def total_force(self) -> np.ndarray:
         out = np.zeros(2)
         _abi.check(self.lib, self._h, self.lib.ibpm_get_forces(self._h, None, _abi.dptr(out)))

@@ -133,6 +133,16 @@ int ibpm_get_state(ibpm_handle *h, ibpm_state_view *st);
  * after the device finished the steps.  IBPM_WARN_CG_MAXITER if any CG stopped at maxiter. */
 int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params);
 
+/* The reference's output accessors vorticity!, x_velocity!, y_velocity!
+ * (src/problem.jl:715-866) for one level (1-based), computed on the device so that
+ * only that level is copied back: Γ / hc² ((nx-1) x (ny-1)), (q + q0)_u / hc
+ * ((nx+1) x ny) or (q + q0)_v / hc (nx x (ny+1)), column-major, hc the level's
+ * grid step. */
+#define IBPM_FIELD_VORTICITY 0
+#define IBPM_FIELD_X_VELOCITY 1
+#define IBPM_FIELD_Y_VELOCITY 2
+int ibpm_get_field(ibpm_handle *h, int32_t field, int32_t level, double *out);
+
 /* state.fb (npanel x 2) and boundary_total_force over all panels (2); NULL skips. */
 int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force);
 
