@@ -171,9 +171,10 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
     """CG iterations and steps/s of the moving-body case (the 512^2 x 4-level
     pitching and plunging plate, 101 points, Re 500, dt 0.002, CG to an absolute
     residual of 1e-10) at a held-out reduced frequency k = 0.55, with the
-    reference's start (the previous solution), the extrapolated start and the
-    learned start; the network is trained on samples of k = 0.25, 0.45, 0.65 and
-    0.85 generated by the solver (after a 60-step start-up)."""
+    reference's start (the previous solution), the extrapolated start, the
+    learned start and the projection onto the last 16 solutions; the network is
+    trained on samples of k = 0.25, 0.45, 0.65 and 0.85 generated by the solver
+    (after a 60-step start-up)."""
     import torch
 
     cg = dict(reltol=0.0, abstol=1e-10, maxiter=5000)
@@ -191,10 +192,10 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
                              net.train(X, T, epochs=200, batch=64, lr=2e-4, seed=8)])
     t_train = time.perf_counter() - t0
     out = {}
-    for mode in ("previous", "extrapolated", "learned"):
+    for mode in ("previous", "extrapolated", "learned", "projected"):
         s = make(0.55)
         if mode != "previous":
-            s.set_warm_start(net if mode == "learned" else None, mode=mode)
+            s.set_warm_start(net if mode == "learned" else None, mode=mode, depth=16)
         for _ in range(60):  # start-up transient, excluded
             s.advance_()
         stream = torch.cuda.ExternalStream(s.stream_handle())

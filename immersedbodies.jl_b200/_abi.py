@@ -97,12 +97,12 @@ EXPORTS = {
     "ibpm_net_train": (C.c_int, [C.c_void_p, _fp, _fp, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                  C.c_uint64, _fp]),
     "ibpm_net_last_error": (C.c_char_p, [C.c_void_p]),
-    "ibpm_set_warm_start": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "ibpm_set_warm_start": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
     "ibpm_warm_start_sample": (C.c_int, [C.c_void_p, _fp, _fp, _fp]),
     "ibpm_lap_inv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ibpm_noalloc_last_error": (C.c_char_p, []),
 }
-IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED = 0, 1, 2
+IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED, IBPM_WS_PROJECTED = 0, 1, 2, 3
 KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5}
 
 _lib = None

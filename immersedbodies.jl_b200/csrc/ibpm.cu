@@ -125,7 +125,7 @@ struct ibpm_handle {
     virtual void diag_binv(double *out) = 0;
     virtual void diag_vort2flux(double *gamma, double *psi, double *q) = 0;
     virtual void diag_reg(const double *f, double *gamma1, const double *q1, double *fout) = 0;
-    virtual void set_warm_start(ibpm_net *net, int mode) = 0;
+    virtual void set_warm_start(ibpm_net *net, int mode, int depth) = 0;
     virtual void warm_start_sample(float *features, float *target, float *prediction) = 0;
 };
 
@@ -187,6 +187,8 @@ struct Engine final : ibpm_handle {
     // of two steps back, the features and prediction of the current step
     ibpm_net *ws = nullptr;
     int ws_mode = IBPM_WS_PREVIOUS;
+    int ws_depth = 0;                       // previous solutions kept for IBPM_WS_PROJECTED
+    double *ws_hist = nullptr, *ws_bhist = nullptr, *ws_G = nullptr, *ws_h = nullptr;
     double *Fprev = nullptr, *ws_z = nullptr, *ws_bz = nullptr, *ws_x2 = nullptr, *ws_bx2 = nullptr;
     float *ws_feat = nullptr, *ws_y = nullptr, *ws_act = nullptr;
     size_t ws_act_cap = 0;
@@ -249,6 +251,23 @@ struct Engine final : ibpm_handle {
             allocs.erase(it);
         }
         cudaFree(p);
+    }
+    // grows the column-batch buffers to kb columns (the projected warm start
+    // applies B to all kept solutions in one batched pass)
+    void grow_batch_buffers(int kb) {
+        if (kb <= kbatch) return;
+        CK(cudaStreamSynchronize(st));
+        for (void *p : {(void *)t1, (void *)t2, (void *)patch, (void *)Gw, (void *)psiw, (void *)qw, (void *)fcol})
+            dfree(p);
+        kbatch = kb;
+        const int k2 = std::max(kbatch, L);
+        t1 = dalloc<T>(ng * k2);
+        t2 = dalloc<T>(ng * k2);
+        patch = dalloc<T>(patch_stride * kbatch);
+        Gw = dalloc<T>(ng * L * kbatch);
+        psiw = dalloc<T>(ng * L * kbatch);
+        qw = dalloc<T>(nq * kbatch);
+        fcol = dalloc<double>(2 * (size_t)np * kbatch);
     }
     // After the B^-1 setup a static-body handle applies B to one vector at a time:
     // the setup's column-batch buffers shrink to one column.
@@ -539,7 +558,7 @@ struct Engine final : ibpm_handle {
     void set_state(const ibpm_state_view *s) override;
     void get_field(int field, int level, double *out) override;
     double *field_d = nullptr;  // one level of an output field
-        void set_warm_start(ibpm_net *net, int mode) override;
+        void set_warm_start(ibpm_net *net, int mode, int depth) override;
     void warm_start_sample(float *features, float *target, float *prediction) override;
     void get_state(ibpm_state_view *s) override;
     bool advance(int64_t nsteps, const ibpm_step_params *params) override;
@@ -955,7 +974,7 @@ void Engine<T>::cg_collect() {
     last_cg_iters = err_h[2];
     last_cg_res = cg_s_h[0];
     first_cg_res = cg_s_h[4];
-    ws_coef[0] = ws_mode != IBPM_WS_PREVIOUS ? cg_s_h[5] : 0.0;
+    ws_coef[0] = ws_mode != IBPM_WS_PREVIOUS ? cg_s_h[5] : 0.0;  // projected: directions kept
     ws_coef[1] = ws_mode == IBPM_WS_LEARNED ? cg_s_h[6] : 0.0;
     if (last_cg_iters >= opt.cg_maxiter) cg_hit_maxiter = true;
     if (err_h[3]) {
@@ -1077,6 +1096,14 @@ void Engine<T>::step_body() {
         check_launch();
         if (ws_mode == IBPM_WS_PREVIOUS) {
             cg(Fbt, Ftmp);
+        } else if (ws_mode == IBPM_WS_PROJECTED) {
+            // Galerkin over the last ws_depth solutions, B applied to all in one batch
+            apply_B(ws_hist, ws_bhist, 2 * np, ws_depth);
+            launch_ws_projection(ws_hist, ws_bhist, Ftmp, Fbt, cg_c, 2 * np, ws_depth, ws_G, ws_h, cg_s + 5, st);
+            check_launch();
+            cg(Fbt, Ftmp, true);
+            launch_ws_shift(ws_hist, Fbt, 2 * np, ws_depth, st);
+            check_launch();
         } else {
             apply_B(ws_z, ws_bz, 2 * np, 2);
             launch_ws_galerkin(ws_z, ws_bz, Ftmp, Fbt, cg_c, ws_x2, ws_bx2, np, 1, cg_s + 5, st);
@@ -1259,11 +1286,26 @@ void Engine<T>::get_field(int field, int level, double *out) {
 }
 
 template <class T>
-void Engine<T>::set_warm_start(ibpm_net *net, int mode) {
+void Engine<T>::set_warm_start(ibpm_net *net, int mode, int depth) {
     CK(cudaSetDevice(device));
     if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
-    if (mode != IBPM_WS_PREVIOUS && mode != IBPM_WS_LEARNED && mode != IBPM_WS_EXTRAPOLATED)
+    if (mode != IBPM_WS_PREVIOUS && mode != IBPM_WS_LEARNED && mode != IBPM_WS_EXTRAPOLATED &&
+        mode != IBPM_WS_PROJECTED)
         throw ApiError{IBPM_ERR_INVALID, "unknown warm-start mode"};
+    if (mode == IBPM_WS_PROJECTED) {
+        if (depth < 1 || depth > 16) throw ApiError{IBPM_ERR_INVALID, "projection depth must be 1 .. 16"};
+        grow_batch_buffers(depth);
+        if (!ws_hist) {
+            ws_hist = dalloc<double>(2 * (size_t)np * 16);
+            ws_bhist = dalloc<double>(2 * (size_t)np * 16);
+            ws_G = dalloc<double>(256);
+            ws_h = dalloc<double>(16);
+        }
+        // the history starts from the current solution alone
+        CK(cudaMemsetAsync(ws_hist, 0, sizeof(double) * 2 * np * 16, st));
+        CK(cudaMemcpyAsync(ws_hist, Fbt, sizeof(double) * 2 * np, cudaMemcpyDeviceToDevice, st));
+        ws_depth = depth;
+    }
     if (mode == IBPM_WS_LEARNED && !net) throw ApiError{IBPM_ERR_INVALID, "the learned warm start needs a network"};
     if (mode != IBPM_WS_LEARNED) net = nullptr;
     if (net) {
@@ -1286,7 +1328,7 @@ template <class T>
 void Engine<T>::warm_start_sample(float *features, float *target, float *prediction) {
     CK(cudaSetDevice(device));
     if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
-    if (ws_mode == IBPM_WS_PREVIOUS)
+    if (ws_mode != IBPM_WS_EXTRAPOLATED && ws_mode != IBPM_WS_LEARNED)
         throw ApiError{IBPM_ERR_INVALID, "warm-start samples need the extrapolated or learned mode"};
     std::vector<double> f(2 * np), xe(2 * np);
     double rs = 0.0;
@@ -1331,6 +1373,10 @@ void Engine<T>::set_state(const ibpm_state_view *s) {
     if (s->ub) CK(cudaMemcpyAsync(P.ub, s->ub, np2, cudaMemcpyHostToDevice, st));
     if (s->fbt) CK(cudaMemcpyAsync(Fbt, s->fbt, np2, cudaMemcpyHostToDevice, st));
     if (s->fbt && Fprev) CK(cudaMemcpyAsync(Fprev, Fbt, np2, cudaMemcpyDeviceToDevice, st));
+    if (s->fbt && ws_hist) {
+        CK(cudaMemsetAsync(ws_hist, 0, sizeof(double) * 2 * np * 16, st));
+        CK(cudaMemcpyAsync(ws_hist, Fbt, np2, cudaMemcpyDeviceToDevice, st));
+    }
     fs_last[0] = s->freestream[0];
     fs_last[1] = s->freestream[1];
     // update_vars! (problem.jl:676-685)
@@ -1596,9 +1642,9 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
 
 void ibpm_destroy(ibpm_handle *h) { delete h; }
 
-int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net) {
+int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t depth) {
     if (!h) return IBPM_ERR_INVALID;
-    return guarded(h, [&] { h->set_warm_start(net, mode); });
+    return guarded(h, [&] { h->set_warm_start(net, mode, depth); });
 }
 
 int ibpm_warm_start_sample(ibpm_handle *h, float *features, float *target, float *prediction) {

@@ -414,6 +414,119 @@ __global__ void ws_galerkin_kernel(const double *__restrict__ z, const double *_
     }
 }
 
+// Projection onto previous solutions (Fischer's method for successive right-hand
+// sides).  V = hist[0 .. k) (most recent first, zero when not yet filled),
+// BV = B V.  One warp per entry of the Gram system: G_ij = (v_i.Bv_j + v_j.Bv_i) / 2
+// for i <= j, h_i = v_i.b; entry e < k(k+1)/2 is (i, j) in row-major upper order,
+// then the k entries of h.
+__global__ void ws_gram_kernel(const double *__restrict__ V, const double *__restrict__ BV,
+                               const double *__restrict__ b, int n, int k, double *__restrict__ G,
+                               double *__restrict__ h) {
+    const int e = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int npair = k * (k + 1) / 2;
+    if (e >= npair + k) return;  // uniform across the warp
+    double a = 0.0, c = 0.0;
+    if (e < npair) {
+        int i = 0, r = e;
+        while (r >= k - i) {
+            r -= k - i;
+            ++i;
+        }
+        const int j = i + r;
+        const double *vi = V + (long long)i * n, *vj = V + (long long)j * n;
+        const double *bi = BV + (long long)i * n, *bj = BV + (long long)j * n;
+        for (int t = lane; t < n; t += 32) {
+            a += vi[t] * bj[t];
+            c += vj[t] * bi[t];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            c += __shfl_down_sync(0xffffffffu, c, o);
+        }
+        if (lane == 0) {
+            G[i * k + j] = 0.5 * (a + c);
+            G[j * k + i] = 0.5 * (a + c);
+        }
+    } else {
+        const int i = e - npair;
+        const double *vi = V + (long long)i * n;
+        for (int t = lane; t < n; t += 32) a += vi[t] * b[t];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) h[i] = a;
+    }
+}
+
+// One thread: G y = h by Cholesky in the given order (most recent direction
+// first), dropping a direction whose pivot falls below 1e-10 of its diagonal
+// (zero vectors and directions the earlier ones already span); y_i = 0 for the
+// dropped ones.  Then x = sum y_i v_i and c = sum y_i B v_i (c = B x for the CG).
+constexpr int kWsMaxDepth = 16;
+__global__ void ws_project_kernel(const double *__restrict__ V, const double *__restrict__ BV,
+                                  const double *__restrict__ G, const double *__restrict__ h, int n, int k,
+                                  double *__restrict__ x, double *__restrict__ c, double *__restrict__ kept) {
+    __shared__ double y[kWsMaxDepth];
+    if (threadIdx.x == 0) {
+        double Lm[kWsMaxDepth][kWsMaxDepth];
+        bool keep[kWsMaxDepth];
+        double z[kWsMaxDepth];
+        int nk = 0;
+        for (int i = 0; i < k; ++i) {
+            keep[i] = false;
+            y[i] = 0.0;
+            const double gii = G[i * k + i];
+            if (!(gii > 0.0)) continue;
+            for (int j = 0; j < i; ++j) {
+                if (!keep[j]) continue;
+                double sm = G[i * k + j];
+                for (int l = 0; l < j; ++l)
+                    if (keep[l]) sm -= Lm[i][l] * Lm[j][l];
+                Lm[i][j] = sm / Lm[j][j];
+            }
+            double d = gii;
+            for (int l = 0; l < i; ++l)
+                if (keep[l]) d -= Lm[i][l] * Lm[i][l];
+            if (d > 1e-10 * gii && isfinite(d)) {
+                Lm[i][i] = sqrt(d);
+                keep[i] = true;
+                ++nk;
+            }
+        }
+        for (int i = 0; i < k; ++i) {  // L z = h
+            if (!keep[i]) continue;
+            double sm = h[i];
+            for (int l = 0; l < i; ++l)
+                if (keep[l]) sm -= Lm[i][l] * z[l];
+            z[i] = sm / Lm[i][i];
+        }
+        for (int i = k - 1; i >= 0; --i) {  // L^T y = z
+            if (!keep[i]) continue;
+            double sm = z[i];
+            for (int l = i + 1; l < k; ++l)
+                if (keep[l]) sm -= Lm[l][i] * y[l];
+            y[i] = sm / Lm[i][i];
+        }
+        if (kept) *kept = (double)nk;
+    }
+    __syncthreads();
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        double xv = 0.0, cv = 0.0;
+        for (int i = 0; i < k; ++i) {
+            xv += y[i] * V[(long long)i * n + t];
+            cv += y[i] * BV[(long long)i * n + t];
+        }
+        x[t] = xv;
+        c[t] = cv;
+    }
+}
+
+// hist[j] <- hist[j-1] for j = k-1 .. 1, hist[0] <- f (vectors of n doubles).
+__global__ void ws_shift_kernel(double *__restrict__ hist, const double *__restrict__ f, int n, int k) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        for (int j = k - 1; j > 0; --j) hist[(long long)j * n + t] = hist[(long long)(j - 1) * n + t];
+        hist[t] = f[t];
+    }
+}
+
 // ---- host-side passes ----
 
 size_t act_floats(const ibpm_net *net, int B, int n) {
@@ -512,6 +625,17 @@ void launch_ws_prediction(const float *y, const ibpm_net *net, int np, double *p
 void launch_ws_galerkin(const double *z, const double *bz, const double *b, double *x, double *c, double *x2,
                         double *c2, int np, int k, double *coef, cudaStream_t st) {
     ws_galerkin_kernel<<<1, 256, 0, st>>>(z, bz, b, x, c, x2, c2, np, k, coef);
+}
+
+void launch_ws_projection(const double *V, const double *BV, const double *b, double *x, double *c, int n, int k,
+                          double *G, double *h, double *kept, cudaStream_t st) {
+    const int items = k * (k + 1) / 2 + k;
+    ws_gram_kernel<<<(items * 32 + 255) / 256, 256, 0, st>>>(V, BV, b, n, k, G, h);
+    // the solve runs on thread 0 of block 0; every block then forms its share of x and c
+    ws_project_kernel<<<1, 256, 0, st>>>(V, BV, G, h, n, k, x, c, kept);
+}
+void launch_ws_shift(double *hist, const double *f, int n, int k, cudaStream_t st) {
+    ws_shift_kernel<<<(n + 255) / 256, 256, 0, st>>>(hist, f, n, k);
 }
 
 }  // namespace ibpm

@@ -43,6 +43,16 @@ void launch_ws_prediction(const float *y, const ibpm_net *net, int np, double *p
 void launch_ws_galerkin(const double *z, const double *bz, const double *b, double *x, double *c, double *x2,
                         double *c2, int np, int k, double *coef, cudaStream_t st);
 
+// Projection onto previous solutions: V = [v_0 .. v_(k-1)] (k <= 16, most recent
+// first, zero vectors allowed), BV = B V, vectors of n doubles.  x <- the
+// combination of V minimising the B-energy norm of the error (Galerkin over
+// span V, with near-dependent directions dropped), c <- B x; G (k x k), h (k)
+// are scratch; kept (optional) receives the number of directions used.
+void launch_ws_projection(const double *V, const double *BV, const double *b, double *x, double *c, int n, int k,
+                          double *G, double *h, double *kept, cudaStream_t st);
+// hist[j] <- hist[j-1] (j = k-1 .. 1), hist[0] <- f.
+void launch_ws_shift(double *hist, const double *f, int n, int k, cudaStream_t st);
+
 // Floats of activation scratch a forward pass of batch B over n points needs.
 size_t net_act_floats(const ibpm_net *net, int B, int n);
 // Forward pass on the device on stream st: x [B][cin][n] (raw features,

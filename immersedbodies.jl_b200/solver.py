@@ -232,15 +232,17 @@ class GpuCnabSolver(AbstractSolver):
         _abi.check(self.lib, self._h, self.lib.ibpm_diag_reg(self._h, None, None, _abi.dptr(q1), _abi.dptr(out)))
         return out
 
-    def set_warm_start(self, net=None, mode: Optional[str] = None):
+    def set_warm_start(self, net=None, mode: Optional[str] = None, depth: int = 8):
         """CG initial guess of this moving-body solver: "previous" (the reference's
-        start from the previous F~b), "learned" (along a `WarmStartNet`'s predicted
-        change; the default when net is given) or "extrapolated" (along the last
-        change F1 - F2).  Keep the network alive while it is installed."""
+        start from the previous F~b), "extrapolated" (Galerkin step along the last
+        change F1 - F2), "learned" (then along a `WarmStartNet`'s correction; the
+        default when net is given) or "projected" (Galerkin over the last `depth`
+        solutions).  Keep the network alive while it is installed."""
         mode = mode or ("learned" if net is not None else "previous")
         m = {"previous": _abi.IBPM_WS_PREVIOUS, "learned": _abi.IBPM_WS_LEARNED,
-             "extrapolated": _abi.IBPM_WS_EXTRAPOLATED}[mode]
-        _abi.check(self.lib, self._h, self.lib.ibpm_set_warm_start(self._h, m, net.handle if net is not None else None))
+             "extrapolated": _abi.IBPM_WS_EXTRAPOLATED, "projected": _abi.IBPM_WS_PROJECTED}[mode]
+        _abi.check(self.lib, self._h, self.lib.ibpm_set_warm_start(self._h, m, net.handle if net is not None else None,
+                                                                    depth))
         self._warm_net = net
 
     def warm_start_sample(self, prediction: bool = False):

@@ -108,7 +108,8 @@ typedef struct ibpm_info {
     int64_t device_bytes;       /* device memory held by the handle */
     double first_cg_residual;   /* ||r0|| of the last step's CG, from its initial guess */
     double warm_start_coef[2];  /* the last step's warm-start Galerkin coefficients: along
-                                   F1 - F2, then along the network's correction */
+                                   F1 - F2, then along the network's correction (the
+                                   projected mode: directions kept, then 0) */
 } ibpm_info;
 
 typedef struct ibpm_handle ibpm_handle;
@@ -246,18 +247,23 @@ int ibpm_net_train(ibpm_net *net, const float *x, const float *t, int64_t nsampl
 const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed create */
 /* Chooses the CG initial guess of a moving-body handle.  F1, F2 are the last two
  * solutions:
- *   IBPM_WS_PREVIOUS      F1 (the reference; net ignored)
+ *   IBPM_WS_PREVIOUS      F1 (the reference; net and depth ignored)
  *   IBPM_WS_EXTRAPOLATED  x_e = F1 + y (F1 - F2)
  *   IBPM_WS_LEARNED       x_e + a p, p the network's correction from x_e's residual
  *                         (net: 10 -> 2 channels on the handle's device, kept alive
  *                         while installed)
- * where y and a minimise the B-energy norm of the error along their directions
- * (Galerkin steps; B is applied to [F1 | F1 - F2] in one batched pass and once
- * more to p; CG reuses B x0). */
+ *   IBPM_WS_PROJECTED     the combination of the last `depth` (1 .. 16) solutions
+ *                         (projection for successive right-hand sides); the history
+ *                         restarts from the current solution when the mode or the
+ *                         state is set
+ * where the coefficients minimise the B-energy norm of the error over their
+ * directions (Galerkin steps with B of the current step, applied in batched
+ * passes; CG reuses B x0). */
 #define IBPM_WS_PREVIOUS 0
 #define IBPM_WS_LEARNED 1
 #define IBPM_WS_EXTRAPOLATED 2
-int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net);
+#define IBPM_WS_PROJECTED 3
+int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t depth);
 /* The last step's warm-start features (10 x npanel floats), target (2 x
  * npanel: the converged F~b minus the extrapolated guess x_e) and, in the
  * learned mode, the network's correction as the step used it (zeros

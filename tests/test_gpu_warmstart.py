@@ -84,16 +84,20 @@ def _iters(s, n):
 
 def test_every_start_reaches_the_same_forces(ib):
     forces, iters = {}, {}
-    for mode in ("previous", "extrapolated"):
+    for mode in ("previous", "extrapolated", "projected"):
         s = _plate(ib, 0.5)
         if mode != "previous":
-            s.set_warm_start(None, mode=mode)
+            s.set_warm_start(None, mode=mode, depth=8)
         iters[mode] = _iters(s, 40)
         forces[mode] = s.total_force().copy()
+        if mode == "projected":
+            assert s.info().warm_start_coef[0] >= 2  # directions kept by the projection
         del s
     f0 = forces["previous"]
-    assert np.abs(forces["extrapolated"] - f0).max() <= 1e-6 * np.abs(f0).max()
-    assert iters["extrapolated"][5:].mean() < iters["previous"][5:].mean()
+    for mode in ("extrapolated", "projected"):
+        assert np.abs(forces[mode] - f0).max() <= 1e-6 * np.abs(f0).max(), mode
+    assert iters["extrapolated"][10:].mean() < iters["previous"][10:].mean()
+    assert iters["projected"][10:].mean() < iters["extrapolated"][10:].mean()
 
 
 def test_learned_warm_start_on_a_held_out_frequency(ib, capsys):
@@ -140,6 +144,8 @@ def test_warm_start_errors(ib):
     s = _plate(ib, 0.5)
     with pytest.raises(ib._abi.IbpmError, match="needs a network"):
         s.set_warm_start(None, mode="learned")
+    with pytest.raises(ib._abi.IbpmError, match="depth"):
+        s.set_warm_start(None, mode="projected", depth=17)
     s.advance_()
     with pytest.raises(ib._abi.IbpmError, match="extrapolated or learned"):
         s.warm_start_sample()
