@@ -21,7 +21,7 @@ using ImmersedBodies: State, Problem, CNAB, AbstractSolver, StaticBody, MovingRi
     MovingGrid, n_panels, timestep, gridstep, inc_time_index!, set_time_index!, update_vars!
 import ImmersedBodies: advance!, getstate, create_solver
 
-export GpuCnabSolver, sync!
+export GpuCnabSolver, sync!, level_vorticity, level_x_velocity, level_y_velocity, set_warm_start!
 
 const libibpm = get(ENV, "IBPM_B200_LIB", joinpath(@__DIR__, "..", "lib", "libibpm_b200.so"))
 
@@ -174,6 +174,32 @@ function advance!(solver::GpuCnabSolver)
         (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}), solver.handle, pointer(fb), C_NULL))
     solver.stale = true
     nothing
+end
+
+# One level of the reference's output fields (vorticity!, x_velocity!, y_velocity!,
+# src/problem.jl:715-866), computed on the device; only that level is copied back.
+function _level_field(solver::GpuCnabSolver, field::Integer, level::Integer, dims)
+    out = Matrix{Float64}(undef, dims...)
+    GC.@preserve out _check(solver.handle, ccall((:ibpm_get_field, libibpm), Cint,
+        (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}), solver.handle, field, level, pointer(out)))
+    out
+end
+_base_n(solver) = solver.state.prob.fluid.grid.base.n
+level_vorticity(solver::GpuCnabSolver, level::Integer=1) =
+    _level_field(solver, 0, level, (_base_n(solver)[1] - 1, _base_n(solver)[2] - 1))
+level_x_velocity(solver::GpuCnabSolver, level::Integer=1) =
+    _level_field(solver, 1, level, (_base_n(solver)[1] + 1, _base_n(solver)[2]))
+level_y_velocity(solver::GpuCnabSolver, level::Integer=1) =
+    _level_field(solver, 2, level, (_base_n(solver)[1], _base_n(solver)[2] + 1))
+
+# CG initial guess for moving bodies: :previous (the reference's start), :extrapolated,
+# or :projected over the last `depth` solutions (1..16); plain CG then runs to the
+# configured tolerance.  (The learned mode needs a network made with ibpm_net_*.)
+function set_warm_start!(solver::GpuCnabSolver, mode::Symbol=:projected; depth::Integer=16)
+    m = Dict(:previous => 0, :extrapolated => 2, :projected => 3)[mode]
+    _check(solver.handle, ccall((:ibpm_set_warm_start, libibpm), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32),
+        solver.handle, m, C_NULL, depth))
+    solver
 end
 
 end # module
