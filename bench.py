@@ -141,6 +141,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(v: float, pg, device) -> float:
+    """The largest v over all ranks; every rank calls it at the same point (pg is
+    torch.distributed or None for one process; device holds the reduction buffer:
+    "cuda" under NCCL, "cpu" under gloo)."""
+    if pg is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, steps: int, max_ms: float) -> float:
+    """Steps/s of the whole job: every rank ran `steps` steps of its own replica and
+    the slowest rank took max_ms."""
+    return world * steps / (max_ms / 1000.0)
+
+
 def dist_init():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -340,13 +359,9 @@ def main():
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
     launches = solver.kernel_launches() - launches_a
-    ms = ev0.elapsed_time(ev1)
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), pg, "cuda")
     ms_step = ms / args.steps
-    value = world * args.steps / (ms / 1000.0)
+    value = whole_job_rate(world, args.steps, ms)
 
     # end to end through the public API: per step, params host->device and fb device->host
     if pg:
@@ -359,12 +374,8 @@ def main():
         solver.advance_()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), pg, "cuda")
+    e2e_value = whole_job_rate(world, e2e_steps, e2e_ms)
     h2d = 8 * 8  # StepDev: freestream (2) + grid motion (6) doubles
     d2h = 8 * 2 * prob.bodies.npanel  # fb
 
