@@ -3,10 +3,11 @@
 // Same algorithm as fft_dst.cuh (complex M-point FFT of two packed lines with
 // the sin pre-twiddle and the prefix-scan post-processing), specialised at
 // compile time: the Stockham stages use radix 16 / 8 / 4 butterflies held in
-// registers (three shared-memory round trips for M = 1024 instead of five), all
-// strides and index splits are constants, the shared buffer is padded by one
-// complex per 16 to keep the strided Stockham writes free of bank conflicts,
-// and the post-processing scan runs on warp shuffles with one block barrier.
+// registers (three shared-memory round trips for M = 1024 instead of five), the
+// pre-twiddle is formed in registers from the first stage's reads, all strides
+// and index splits are constants, the shared buffer is padded by one complex per
+// 16 to keep the strided Stockham writes free of bank conflicts, and the
+// post-processing scan runs on warp shuffles with one block barrier.
 // T (double or float) is the element type; the scan accumulates in double.
 #pragma once
 #include "fft_dst.cuh"
@@ -299,44 +300,6 @@ struct Pow2Dst {
     static __host__ __device__ constexpr int smem_len(int) { return padded_len(M); }
 
     static __device__ __forceinline__ int idx(int i) { return pad16(i); }
-
-    static __device__ __forceinline__ void fft(C *buf, const C *__restrict__ tw, int t) {
-        constexpr int N1 = P::R0, N2 = N1 * P::R1, N3 = N2 * P::R2, N4 = N3 * P::R3;
-        static_assert(N4 * P::R4 == M, "plan must factor M");
-        stage_ct<M, P::R0, 1, TPF, C>(buf, tw, t);
-        stage_ct<M, P::R1, N1, TPF, C>(buf, tw, t);
-        stage_ct<M, P::R2, N2, TPF, C>(buf, tw, t);
-        if constexpr (P::R3 > 1) stage_ct<M, P::R3, N3, TPF, C>(buf, tw, t);
-        if constexpr (P::R4 > 1) stage_ct<M, P::R4, N4, TPF, C>(buf, tw, t);
-    }
-
-    // pre-twiddle in place; buf[1..M-1] hold z, buf[0], buf[M] are read as 0
-    static __device__ __forceinline__ void pre(C *buf, const T *__restrict__ sn, int t) {
-        constexpr int H = M / 2;
-        constexpr int NIT = (H + 1 + TPF - 1) / TPF;
-        T s[NIT];
-#pragma unroll
-        for (int k = 0; k < NIT; ++k) {  // issue the table loads first
-            const int j = t + k * TPF;
-            s[k] = j <= H ? __ldg(&sn[j]) : (T)0;
-        }
-#pragma unroll
-        for (int k = 0; k < NIT; ++k) {
-            const int j = t + k * TPF;
-            if (j > H) break;
-            if (j == 0) {
-                buf[0] = Cx<T>::make(0, 0);
-            } else if (j == H) {
-                const C z = buf[pad16(H)];
-                buf[pad16(H)] = s[k] * (z + z);
-            } else {
-                const C a = buf[pad16(j)], b = buf[pad16(M - j)];
-                buf[pad16(j)] = s[k] * (a + b) + (T)0.5 * (a - b);
-                buf[pad16(M - j)] = s[k] * (a + b) + (T)0.5 * (b - a);
-            }
-        }
-        __syncthreads();
-    }
 
     // post-processing: V in buf[0..M) -> y in buf[1..M-1]; buf[0] = buf[M] = 0.
     // Thread t owns the E = H/TPF consecutive k in [t E, t E + E): a sequential
