@@ -947,3 +947,10 @@ int orc_binv(orc_solver *s, double *out) {
     memcpy(out, s->Binv, sizeof(double) * n * n);
     return 1;
 }
+
+int orc_set_binv(orc_solver *s, const double *in) {
+    if (!s->Binv) return 0;
+    const size_t n = 2 * (size_t)s->np;
+    memcpy(s->Binv, in, sizeof(double) * n * n);
+    return 1;
+}

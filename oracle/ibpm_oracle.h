@@ -89,6 +89,9 @@ void orc_set_t0(orc_solver *s, double t0);
 int orc_last_cg_iters(orc_solver *s);
 /* Copy of the precomputed B^-1 (2np x 2np column-major) for static bodies; returns 0 if absent. */
 int orc_binv(orc_solver *s, double *out);
+/* Replaces the precomputed B^-1 of static bodies (2np x 2np, column-major), e.g.
+ * in a timing_only solver that skipped building it; 0 when there is none. */
+int orc_set_binv(orc_solver *s, const double *in);
 /* Apply the Schur complement B (src/coupling.jl:150-177) with the current weights. */
 void orc_apply_B(orc_solver *s, double *x, const double *z);
 /* vort2flux! on caller arrays (src/fluid.jl:175-206); Gamma is coarsified in place. */

@@ -71,6 +71,8 @@ def load():
     lib.orc_last_cg_iters.argtypes = [C.c_void_p]
     lib.orc_binv.restype = C.c_int
     lib.orc_binv.argtypes = [C.c_void_p, _dp]
+    lib.orc_set_binv.restype = C.c_int
+    lib.orc_set_binv.argtypes = [C.c_void_p, _dp]
     lib.orc_apply_B.argtypes = [C.c_void_p, _dp, _dp]
     lib.orc_vort2flux.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.orc_reg_rot.argtypes = [C.c_void_p, _dp, _dp]
@@ -259,6 +261,12 @@ class OracleSolver:
         n = 2 * self.state.prob.bodies.npanel
         out = np.empty((n, n), order="F")
         return out if self.lib.orc_binv(self._h, _p(out)) else None
+
+    def set_binv(self, m):
+        """Replaces the precomputed B^-1 (static bodies) with m (2np x 2np)."""
+        m = np.asfortranarray(m, dtype=np.float64)
+        if not self.lib.orc_set_binv(self._h, _p(m)):
+            raise ValueError("this solver has no precomputed B^-1")
 
     def apply_B(self, z):
         z = np.ascontiguousarray(z, dtype=np.float64)

@@ -21,7 +21,7 @@ def _lams(orc, prob, op, level):
     return 1 + lam * prob.scheme.dt / den
 
 
-@pytest.mark.parametrize("n", [32, 40, 48, 64, 150, 200, 256, 384])
+@pytest.mark.parametrize("n", [32, 40, 48, 64, 150, 200, 256, 384, 512, 1024])
 @pytest.mark.parametrize("op", [0, 1, 2])
 def test_solve_matches_oracle(ib, orc, n, op):
     prob = ib.configs.small_cylinder(n, 2)

@@ -136,3 +136,26 @@ def test_gpu_deterministic(ib):
         s.getstate()
         out.append((st.Gamma.copy(), st.fb.copy()))
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_benchmark_case_steps_match_oracle(ib, orc):
+    """The benchmark workload itself -- the 1024 x 1024, 5-level cylinder with seeded
+    noise, where the compile-time 1024-point transforms run -- for 2 steps against
+    the oracle.  Building B^-1 on the CPU at this size takes minutes, so the oracle
+    is given the GPU's B^-1 (checked against the oracle's own on smaller grids)."""
+    prob = ib.configs.cylinder_re100_1024()
+    sg = ib.configs.seed_vorticity(ib.State(prob))
+    so = ib.configs.seed_vorticity(ib.State(prob))
+    gpu = ib.create_solver(sg)
+    cpu = orc.OracleSolver(so, timing_only=True)
+    cpu.set_binv(gpu.diag_binv())
+    for _ in range(2):
+        gpu.advance_()
+        cpu.advance_(pull=False)
+    cpu.pull()
+    gpu.getstate()
+    assert rel_l2(sg.Gamma, so.Gamma) <= TOL_GAMMA
+    assert rel_l2(sg.q, so.q) <= TOL_GAMMA
+    assert rel_l2(sg.psi, so.psi) <= TOL_GAMMA
+    cd_g, cd_o = 2 * sg.fb.sum(axis=0), 2 * so.fb.sum(axis=0)
+    assert np.abs(cd_g - cd_o).max() <= TOL_FORCE * max(1.0, np.abs(cd_o).max())
