@@ -157,6 +157,11 @@ struct DftC<16, C> {
     }
 };
 
+template <class C>
+struct DftC<3, C> {
+    static __device__ __forceinline__ void run(C *v) { Dft<3, C>::run(v); }
+};
+
 // ---- compile-time plans ----
 // Every stage has NB = M/R butterflies with NB % 16 == 0 and a stride NS that
 // is 1 or a multiple of 16, so all padded shared-memory offsets of a stage are
@@ -288,6 +293,88 @@ __device__ __forceinline__ void stage_first_pre(C *buf, const T *__restrict__ sn
     __syncthreads();
 }
 
+// A Stockham stage with compile-time sizes for any radix and stride: the same
+// butterflies as stage_ct, with the padded shared-memory index computed for
+// every element (strides with a factor 3 do not keep the pads at constant
+// offsets).  Butterfly j < M/R takes inputs j + r M/R and writes outputs
+// (j / NS) NS R + j % NS + r NS.
+template <int M, int R, int NS, int TPF, class C>
+__device__ __forceinline__ void stage_gen(C *buf, const C *__restrict__ tw, int t) {
+    constexpr int NB = M / R;
+    constexpr int K = (NB + TPF - 1) / TPF;
+    constexpr int TWS = M / (NS * R);
+    C v[K][R];
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (j >= NB) break;
+        const int k = j % NS;
+        C w[R];
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) w[r] = __ldg(&tw[r * k * TWS]);
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[kb][r] = buf[pad16(j + r * NB)];
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[kb][r] = cmul(v[kb][r], w[r]);
+        }
+        DftC<R, C>::run(v[kb]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (j >= NB) break;
+        const int base = (j / NS) * NS * R + j % NS;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[pad16(base + r * NS)] = v[kb][r];
+    }
+    __syncthreads();
+}
+
+// stage_gen's first stage (NS = 1) with the DST pre-twiddle folded into its reads,
+// as stage_first_pre.
+template <int M, int R, int TPF, class C, class T>
+__device__ __forceinline__ void stage_gen_first_pre(C *buf, const T *__restrict__ sn, int t) {
+    constexpr int NB = M / R;
+    constexpr int K = (NB + TPF - 1) / TPF;
+    constexpr int H = M / 2;
+    T s[K][R];
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int n = j + r * NB;
+            s[kb][r] = j < NB ? __ldg(&sn[n <= H ? n : M - n]) : (T)0;
+        }
+    }
+    C v[K][R];
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (j >= NB) break;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int n = j + r * NB;
+            const C a = buf[pad16(n)], b = buf[pad16(M - n)];
+            v[kb][r] = n == 0 ? Cx<T>::make(0, 0) : s[kb][r] * (a + b) + (T)0.5 * (a - b);
+        }
+        DftC<R, C>::run(v[kb]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kb = 0; kb < K; ++kb) {
+        const int j = t + kb * TPF;
+        if (j >= NB) break;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[pad16(j * R + r)] = v[kb][r];
+    }
+    __syncthreads();
+}
+
 template <int M, class T, class PL = Pow2Plan<M>>
 struct Pow2Dst {
     using P = PL;
@@ -372,6 +459,34 @@ struct Pow2Dst {
     static __device__ __forceinline__ void dst(C *buf, const PlanT<T> &pl, int t, double2 *wt) {
         fft_pre(buf, pl.tw, pl.sn, t);
         post(buf, t, wt);
+    }
+};
+
+// Compile-time transforms for lengths with a factor 3 (M = 384 = 3 x 8 x 16):
+// the general stages above, Pow2Dst's scan post-processing.
+template <int M>
+struct MixPlan;
+template <>
+struct MixPlan<384> : PlanCT<64, 3, 8, 16> {};
+
+template <int M, class T, class PL = MixPlan<M>>
+struct MixDst : Pow2Dst<M, T, PL> {
+    using Base = Pow2Dst<M, T, PL>;
+    using C = typename Base::C;
+    using P = PL;
+    static constexpr int TPF = P::TPF;
+    static __device__ __forceinline__ void fft_pre(C *buf, const C *__restrict__ tw, const T *__restrict__ sn, int t) {
+        constexpr int N1 = P::R0, N2 = N1 * P::R1, N3 = N2 * P::R2, N4 = N3 * P::R3;
+        static_assert(N4 * P::R4 == M, "plan must factor M");
+        stage_gen_first_pre<M, P::R0, TPF, C, T>(buf, sn, t);
+        stage_gen<M, P::R1, N1, TPF, C>(buf, tw, t);
+        stage_gen<M, P::R2, N2, TPF, C>(buf, tw, t);
+        if constexpr (P::R3 > 1) stage_gen<M, P::R3, N3, TPF, C>(buf, tw, t);
+        if constexpr (P::R4 > 1) stage_gen<M, P::R4, N4, TPF, C>(buf, tw, t);
+    }
+    static __device__ __forceinline__ void dst(C *buf, const PlanT<T> &pl, int t, double2 *wt) {
+        fft_pre(buf, pl.tw, pl.sn, t);
+        Base::post(buf, t, wt);
     }
 };
 

@@ -330,8 +330,8 @@ struct Engine final : ibpm_handle {
     }
 
     // ---- line passes ----
-    // Dispatch on the transform length: compile-time power-of-two transforms
-    // for M in {128, 256, 512, 1024}, the runtime mixed-radix one otherwise.
+    // Dispatch on the transform length: compile-time transforms for
+    // M in {256, 384, 512, 1024}, the runtime mixed-radix one otherwise.
     template <class D, class In, class Out>
     void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch) {
         const int pairs = (ny - 1 + 1) / 2;
@@ -349,6 +349,7 @@ struct Engine final : ibpm_handle {
             case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch); break;
             case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch); break;
             case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch); break;
+            case 384: xpass_t<MixDst<384, R>>(pl, in, out, nbatch); break;
             default: xpass_t<GenericDst<R>>(pl, in, out, nbatch); break;
         }
         check_launch();
@@ -369,6 +370,7 @@ struct Engine final : ibpm_handle {
             case 1024: ypass_t<Pow2Dst<1024, R>>(pl, in, out, bs, nbatch, m); break;
             case 512: ypass_t<Pow2Dst<512, R>>(pl, in, out, bs, nbatch, m); break;
             case 256: ypass_t<Pow2Dst<256, R>>(pl, in, out, bs, nbatch, m); break;
+            case 384: ypass_t<MixDst<384, R>>(pl, in, out, bs, nbatch, m); break;
             default: ypass_t<GenericDst<R>>(pl, in, out, bs, nbatch, m); break;
         }
         check_launch();
