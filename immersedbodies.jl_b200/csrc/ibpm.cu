@@ -1614,6 +1614,25 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
         return IBPM_ERR_INVALID;
     }
     for (int b = 0; b < p->nbody; ++b)
+        if (p->body_start[b + 1] < p->body_start[b]) {
+            g_create_error = "body_start must not decrease";
+            return IBPM_ERR_INVALID;
+        }
+    if (!std::isfinite(p->h) || !std::isfinite(p->x0) || !std::isfinite(p->y0) || !std::isfinite(p->dt) ||
+        !std::isfinite(p->Re)) {
+        g_create_error = "non-finite grid or fluid parameter";
+        return IBPM_ERR_INVALID;
+    }
+    for (long long k = 0; k < 2LL * p->npanel; ++k)
+        if (!std::isfinite(p->body_xb[k]) || (k < p->npanel && !std::isfinite(p->body_ds[k]))) {
+            g_create_error = "non-finite body point";
+            return IBPM_ERR_INVALID;
+        }
+    if (opt.cg_maxiter < 0 || !(opt.cg_reltol >= 0) || !(opt.cg_abstol >= 0)) {
+        g_create_error = "CG options must be non-negative";
+        return IBPM_ERR_INVALID;
+    }
+    for (int b = 0; b < p->nbody; ++b)
         if (p->body_kind[b] != IBPM_BODY_STATIC && p->body_kind[b] != IBPM_BODY_MOVING_RIGID) {
             g_create_error = "unknown body kind";
             return IBPM_ERR_INVALID;
