@@ -3,6 +3,7 @@
 // (mixed-precision path); arithmetic on boundary values, multipliers and
 // coupling sums is done in double.  Included by ibpm.cu only.
 #pragma once
+#include <type_traits>
 #include "common.cuh"
 #include "fft_pow2.cuh"
 
@@ -48,6 +49,25 @@ struct InBC {
         if (on_ring(g, i, j)) v = apply_bc_at(v, coarse + b * cbs, g, i, j, 1.0);
         return v;
     }
+    // The compile-time X pass loads the field alone (plain()) and then adds the
+    // boundary values to the ring elements (ring()), so the loads of a line are
+    // not held up behind the boundary reads; the sum is the one operator() forms.
+    static constexpr bool kSplitRing = true;
+    __device__ __forceinline__ double plain(int b, int i, int j) const { return (double)gam[b * bs + GI(i, j)]; }
+    __device__ __forceinline__ bool ring_row(int j) const { return j == 1 || j == g.ny - 1; }
+    __device__ __forceinline__ double ring(double v, int b, int i, int j) const {
+        return apply_bc_at(v, coarse + b * cbs, g, i, j, 1.0);
+    }
+};
+
+// detects the split prologue of InBC
+template <class In, class = void>
+struct SplitRing {
+    static constexpr bool value = false;
+};
+template <class In>
+struct SplitRing<In, std::void_t<decltype(In::kSplitRing)>> {
+    static constexpr bool value = In::kSplitRing;
 };
 
 // Prologue rot!(Gamma, reg!(q, f)) (src/fluid.jl:101-111 after src/coupling.jl:72-85),
@@ -146,12 +166,32 @@ __global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
         // before the first shared-memory store
         constexpr int NIT = (D::MC + 1 + TPF - 1) / TPF;
         T za[NIT], zb[NIT];
+        if constexpr (SplitRing<In>::value) {
 #pragma unroll
-        for (int k = 0; k < NIT; ++k) {
-            const int i = t + k * TPF;
-            const bool in_line = i >= 1 && i < D::MC;
-            za[k] = (in_line && va) ? (T)in(b, i, ja) : (T)0;
-            zb[k] = (in_line && vb) ? (T)in(b, i, jb) : (T)0;
+            for (int k = 0; k < NIT; ++k) {
+                const int i = t + k * TPF;
+                const bool in_line = i >= 1 && i < D::MC;
+                za[k] = (in_line && va) ? (T)in.plain(b, i, ja) : (T)0;
+                zb[k] = (in_line && vb) ? (T)in.plain(b, i, jb) : (T)0;
+            }
+            // boundary values on the ring: whole rows 1 and ny-1, the ends of the others
+            const bool ra = va && in.ring_row(ja), rb = vb && in.ring_row(jb);
+#pragma unroll
+            for (int k = 0; k < NIT; ++k) {
+                const int i = t + k * TPF;
+                if (i < 1 || i >= D::MC) continue;
+                const bool end = i == 1 || i == D::MC - 1;
+                if (va && (ra || end)) za[k] = (T)in.ring(in.plain(b, i, ja), b, i, ja);
+                if (vb && (rb || end)) zb[k] = (T)in.ring(in.plain(b, i, jb), b, i, jb);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < NIT; ++k) {
+                const int i = t + k * TPF;
+                const bool in_line = i >= 1 && i < D::MC;
+                za[k] = (in_line && va) ? (T)in(b, i, ja) : (T)0;
+                zb[k] = (in_line && vb) ? (T)in(b, i, jb) : (T)0;
+            }
         }
 #pragma unroll
         for (int k = 0; k < NIT; ++k) {
