@@ -469,7 +469,7 @@ struct Engine final : ibpm_handle {
                 ypass<double>(t1_hi, t2_hi, ng, 1, mult(MULT_LAPINV, 1, 0));
                 xpass<double>(InPlain<double>{t2_hi, ng, nx - 1}, OutPlain<double>{psi1_hi, ng, nx - 1}, 1);
                 const dim3 blk(64, 4);
-                const dim3 grd((nx + 1 + 63) / 64, (ny + 3) / 4 + (ny + 1 + 3) / 4, 1);
+                const dim3 grd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, 1);
                 curl_kernel<double, double, T><<<grd, blk, 0, st>>>(qs1_hi, 0, psi1_hi, 0, coarse, 0, g);
                 check_launch();
                 continue;
@@ -482,7 +482,7 @@ struct Engine final : ibpm_handle {
             xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch);
             if (curl_all || lev == 1) {
                 const dim3 blk(64, 4);
-                const dim3 grd((nx + 1 + 63) / 64, (ny + 3) / 4 + (ny + 1 + 3) / 4, nbatch);
+                const dim3 grd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, nbatch);
                 const int pe = prof_begin();
                 curl_kernel<T, T, T><<<grd, blk, 0, st>>>(qout + (lev - 1) * nq, qbs, Pl, bs,
                                                           lev < L ? psi_ + lev * ng : nullptr, bs, g);

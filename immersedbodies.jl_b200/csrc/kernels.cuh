@@ -624,25 +624,29 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a
 }
 
 // 4-argument curl! (src/fluid.jl:230-276) with psi_bc = get_bc(psi_coarse) (zero if null).
-// A 2D grid over the faces: blockIdx.y < ceil((ny+1)/by) covers the x faces
-// (rows j <= ny) and, offset by that count, the y faces (rows j <= ny+1).
-// Batch b (blockIdx.z) uses psi + b*bs, q + b*qbs, coarse + b*cbs.
+// One thread per (i, j) writes both faces there: the x face u(i, j) (i <= nx+1,
+// j <= ny) and the y face v(i, j) (i <= nx, j <= ny+1); inside the ring they share
+// psi(i-1, j-1).  Batch b (blockIdx.z) uses psi + b*bs, q + b*qbs, coarse + b*cbs.
 template <class T, class TP, class TC>
 __global__ void curl_kernel(T *__restrict__ qout, long long qbs, const TP *__restrict__ psi, long long bs,
                             const TC *__restrict__ coarse, long long cbs, Grid g) {
     const int nx = g.nx, ny = g.ny;
     const long long nu = (long long)(nx + 1) * ny;
-    const int rows_u = (ny + blockDim.y - 1) / blockDim.y;
-    const bool yface = (int)blockIdx.y >= rows_u;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = (yface ? blockIdx.y - rows_u : blockIdx.y) * blockDim.y + threadIdx.y + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int b = blockIdx.z;
+    if (i > nx + 1 || j > ny + 1) return;
     const TP *Pt = psi + b * bs;
     const TC *C = coarse ? coarse + b * cbs : nullptr;
     T *q = qout + b * qbs;
     auto P = [&](long long k) -> double { return (double)Pt[k]; };
-    if (!yface) {
-        if (i > nx + 1 || j > ny) return;
+    if (i >= 2 && i <= nx - 1 && j >= 2 && j <= ny - 1) {
+        const double pc = P(GI(i - 1, j - 1));
+        q[UI(i, j)] = (T)(P(GI(i - 1, j)) - pc);
+        q[VI(i, j)] = (T)(pc - P(GI(i, j - 1)));
+        return;
+    }
+    if (j <= ny) {
         double v;
         if (i == 1)
             v = getbc(C, g, SIDE_L, j + 1) - getbc(C, g, SIDE_L, j);
@@ -655,8 +659,8 @@ __global__ void curl_kernel(T *__restrict__ qout, long long qbs, const TP *__res
         else
             v = P(GI(i - 1, j)) - P(GI(i - 1, j - 1));
         q[UI(i, j)] = (T)v;
-    } else {
-        if (i > nx || j > ny + 1) return;
+    }
+    if (i <= nx) {
         double v;
         if (j == 1)
             v = getbc(C, g, SIDE_B, i) - getbc(C, g, SIDE_B, i + 1);
