@@ -181,8 +181,9 @@ __global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
                 const int i = t + k * TPF;
                 if (i < 1 || i >= D::MC) continue;
                 const bool end = i == 1 || i == D::MC - 1;
-                if (va && (ra || end)) za[k] = (T)in.ring(in.plain(b, i, ja), b, i, ja);
-                if (vb && (rb || end)) zb[k] = (T)in.ring(in.plain(b, i, jb), b, i, jb);
+                // za[k] holds the field value exactly ((T)(double)x == x), so no reload
+                if (va && (ra || end)) za[k] = (T)in.ring((double)za[k], b, i, ja);
+                if (vb && (rb || end)) zb[k] = (T)in.ring((double)zb[k], b, i, jb);
             }
         } else {
 #pragma unroll
