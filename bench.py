@@ -191,9 +191,11 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
     pitching and plunging plate, 101 points, Re 500, dt 0.002, CG to an absolute
     residual of 1e-10) at a held-out reduced frequency k = 0.55, with the
     reference's start (the previous solution), the extrapolated start, the
-    learned start and the projection onto the last 16 solutions; the network is
+    learned start, the projection onto the last 16 solutions and the direct start
+    (B assembled and inverted on the GPU every step, or every 8th); the network is
     trained on samples of k = 0.25, 0.45, 0.65 and 0.85 generated by the solver
-    (after a 60-step start-up)."""
+    (after a 60-step start-up).  Every run takes the same steps, so their final
+    forces differ only by the CG tolerance."""
     import torch
 
     cg = dict(reltol=0.0, abstol=1e-10, maxiter=5000)
@@ -210,11 +212,13 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
     losses = np.concatenate([net.train(X, T, epochs=200, batch=64, lr=1e-3),
                              net.train(X, T, epochs=200, batch=64, lr=2e-4, seed=8)])
     t_train = time.perf_counter() - t0
-    out = {}
-    for mode in ("previous", "extrapolated", "learned", "projected"):
+    out, forces = {}, {}
+    runs = (("previous", "previous", 16), ("extrapolated", "extrapolated", 16), ("learned", "learned", 16),
+            ("projected", "projected", 16), ("direct", "direct", 1), ("direct_every_8", "direct", 8))
+    for label, mode, depth in runs:
         s = make(0.55)
         if mode != "previous":
-            s.set_warm_start(net if mode == "learned" else None, mode=mode, depth=16)
+            s.set_warm_start(net if mode == "learned" else None, mode=mode, depth=depth)
         for _ in range(60):  # start-up transient, excluded
             s.advance_()
         stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -231,14 +235,18 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        out[mode] = {"cg_iterations_mean": float(np.mean(it)), "first_residual_geomean": float(np.exp(np.mean(np.log(r0)))),
-                     "steps_per_s": eval_steps / (ms / 1000.0),
-                     "galerkin_coef_median": [float(v) for v in np.median(np.asarray(coef), axis=0)]}
+        forces[label] = np.asarray(s.total_force(), dtype=np.float64).copy()
+        out[label] = {"cg_iterations_mean": float(np.mean(it)), "first_residual_geomean": float(np.exp(np.mean(np.log(np.maximum(r0, 1e-300))))),
+                      "steps_per_s": eval_steps / (ms / 1000.0),
+                      "galerkin_coef_median": [float(v) for v in np.median(np.asarray(coef), axis=0)]}
         if mode == "learned":
             Xh, Th, _ = ib.warmstart.collect_samples(s, 30)
             ph = net.forward(Xh)
-            out[mode]["held_out_r2"] = float(1 - ((ph - Th) ** 2).sum() / ((Th - Th.mean(axis=(0, 2), keepdims=True)) ** 2).sum())
+            out[label]["held_out_r2"] = float(1 - ((ph - Th) ** 2).sum() / ((Th - Th.mean(axis=(0, 2), keepdims=True)) ** 2).sum())
         del s
+    for label in out:
+        f0 = forces["previous"]
+        out[label]["max_force_diff_vs_previous_rel"] = float(np.abs(forces[label] - f0).max() / np.abs(f0).max())
     base = out["previous"]
     return {"workload": "pitching_plate_512: 512x512 cells x 4 levels, 101-point plate pitching 30 deg and plunging "
                         "0.25 chord, Re 500, dt 0.002; CG to |r| <= 1e-10; held-out k = 0.55",

@@ -188,6 +188,13 @@ struct Engine final : ibpm_handle {
     ibpm_net *ws = nullptr;
     int ws_mode = IBPM_WS_PREVIOUS;
     int ws_depth = 0;                       // previous solutions kept for IBPM_WS_PROJECTED
+    // IBPM_WS_DIRECT: B^-1 of the body position, rebuilt every ws_refresh steps
+    // (ws_since counts the steps since the last rebuild) by its own graph
+    int ws_refresh = 1;
+    long long ws_since = 0;
+    cudaGraph_t binv_graph = nullptr;
+    cudaGraphExec_t binv_exec = nullptr;
+    long long binv_graph_launches = 0;
     double *ws_hist = nullptr, *ws_bhist = nullptr, *ws_G = nullptr, *ws_h = nullptr;
     double *Fprev = nullptr, *ws_z = nullptr, *ws_bz = nullptr, *ws_x2 = nullptr, *ws_bx2 = nullptr;
     float *ws_feat = nullptr, *ws_y = nullptr, *ws_act = nullptr;
@@ -202,7 +209,7 @@ struct Engine final : ibpm_handle {
     long long patch_stride = 0;
     T *Gw = nullptr, *psiw = nullptr, *qw = nullptr;  // batch work (K columns)
     double *fcol = nullptr;
-    double *Binv = nullptr, *rowk = nullptr, *colk = nullptr;
+    double *Binv = nullptr, *Bwork = nullptr;  // B^-1 and the Gauss-Jordan ping-pong buffer
     double *cg_u = nullptr, *cg_r = nullptr, *cg_c = nullptr, *cg_s = nullptr, *cg_s_h = nullptr;
     int *err = nullptr, *err_h = nullptr;
     int last_cg_iters = 0;
@@ -307,6 +314,10 @@ struct Engine final : ibpm_handle {
             graph_exec[p] = nullptr;
             graph[p] = nullptr;
         }
+        if (binv_exec) cudaGraphExecDestroy(binv_exec);
+        if (binv_graph) cudaGraphDestroy(binv_graph);
+        binv_exec = nullptr;
+        binv_graph = nullptr;
     }
     ~Engine() override {
         if (st) cudaStreamSynchronize(st);
@@ -590,6 +601,9 @@ struct Engine final : ibpm_handle {
     void diag_reg(const double *f, double *gamma1, const double *q1, double *fout) override;
     void setup();
     void build_Binv();
+    void assemble_invert_B();
+    void direct_rebuild();
+    int batch_width() const;
     void cg(double *x, const double *b, bool have_bx = false);
     void cg_collect();
     int *cg_it = nullptr;
@@ -700,9 +714,7 @@ void Engine<T>::setup() {
     memset(prm_h, 0, sizeof(StepDev));
     CK(cudaMemcpyAsync(ref_xb_d, ref_xb.data(), sizeof(double) * 2 * np, cudaMemcpyHostToDevice, st));
 
-    // batch width for the B^-1 setup: ~4 GB of column work
-    const long long per_col = (2 * ng * L + nq + 2 * ng) * (long long)sizeof(T);
-    kbatch = (int)std::max(1LL, std::min<long long>(64, (4LL << 30) / per_col));
+    kbatch = batch_width();
     if (!std::is_same<T, double>::value) kbatch = 1;  // FP32 builds B^-1 with an FP64 engine
     if (!static_bodies) kbatch = 2;  // the warm start applies B to two vectors at once
     kbatch = std::min(kbatch, 2 * np);
@@ -779,13 +791,35 @@ void Engine<T>::setup() {
     CK(cudaStreamSynchronize(st));
 }
 
+// Columns of B applied at once when B is assembled: about 4 GB of column work.
+template <class T>
+int Engine<T>::batch_width() const {
+    const long long per_col = (2 * ng * L + nq + 2 * ng) * (long long)sizeof(T);
+    return (int)std::min<long long>(2 * np, std::max(1LL, std::min<long long>(64, (4LL << 30) / per_col)));
+}
+
 // _Binv_precomputed (src/coupling.jl:187-192): B column by column, then its inverse.
 template <class T>
 void Engine<T>::build_Binv() {
     const int n = 2 * np;
     Binv = dalloc<double>((size_t)n * n);
-    rowk = dalloc<double>(n);
-    colk = dalloc<double>(n);
+    Bwork = dalloc<double>((size_t)n * n);
+    assemble_invert_B();
+    CK(cudaMemcpyAsync(err_h, err, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    dfree(Bwork);
+    Bwork = nullptr;
+    if (err_h[1] != 0) throw ApiError{IBPM_ERR_INVALID, "B is not positive definite (pivot " + std::to_string(err_h[1]) + ")"};
+}
+
+// B of the current body position into Binv, kbatch columns per batched
+// application, then inverted by Gauss-Jordan elimination without pivoting
+// between Binv and Bwork (B is positive definite; its multi-level
+// discretisation leaves it symmetric only to about 1e-6 relative); a pivot
+// <= 0 sets err[1].
+template <class T>
+void Engine<T>::assemble_invert_B() {
+    const int n = 2 * np;
     for (int c0 = 0; c0 < n; c0 += kbatch) {
         const int nb = std::min(kbatch, n - c0);
         unit_columns_kernel<<<(n * nb + 255) / 256, 256, 0, st>>>(fcol, n, c0, nb);
@@ -793,14 +827,42 @@ void Engine<T>::build_Binv() {
         apply_B(fcol, Binv + (size_t)c0 * n, n, nb);
     }
     for (int k = 0; k < n; ++k) {
-        gj_save_kernel<<<(n + 255) / 256, 256, 0, st>>>(Binv, n, k, rowk, colk, err + 1);
-        check_launch();
-        gj_update_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(Binv, n, k, rowk, colk);
+        // n = 2 np is even: the last step writes Binv
+        const double *src = (k & 1) ? Bwork : Binv;
+        double *dst = (k & 1) ? Binv : Bwork;
+        gj_step_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(src, dst, n, k, err + 1);
         check_launch();
     }
-    CK(cudaMemcpyAsync(err_h, err, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (err_h[1] != 0) throw ApiError{IBPM_ERR_INVALID, "B is not positive definite (pivot " + std::to_string(err_h[1]) + ")"};
+}
+
+// IBPM_WS_DIRECT's rebuild of B^-1 for the body position of this step, as a graph
+// captured on first use (its buffers stay fixed until drop_graphs).
+template <class T>
+void Engine<T>::direct_rebuild() {
+    if (!use_graphs || prof) {
+        assemble_invert_B();
+        return;
+    }
+    if (!binv_exec) {
+        const long long l0 = launches;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            assemble_invert_B();
+        } catch (...) {
+            cudaGraph_t gdrop = nullptr;
+            cudaStreamEndCapture(st, &gdrop);
+            if (gdrop) cudaGraphDestroy(gdrop);
+            (void)cudaGetLastError();
+            launches = l0;
+            throw;
+        }
+        CK(cudaStreamEndCapture(st, &binv_graph));
+        CK(cudaGraphInstantiate(&binv_exec, binv_graph, 0));
+        binv_graph_launches = launches - l0;
+        launches = l0;
+    }
+    CK(cudaGraphLaunch(binv_exec, st));
+    launches += binv_graph_launches;
 }
 
 namespace {
@@ -971,14 +1033,22 @@ void Engine<T>::cg_collect() {
     CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_h + 2, cg_it, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_h + 3, err + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (ws_mode == IBPM_WS_DIRECT) CK(cudaMemcpyAsync(err_h + 1, err + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     cg_pending = false;
     last_cg_iters = err_h[2];
     last_cg_res = cg_s_h[0];
     first_cg_res = cg_s_h[4];
-    ws_coef[0] = ws_mode != IBPM_WS_PREVIOUS ? cg_s_h[5] : 0.0;  // projected: directions kept
+    // projected: directions kept; extrapolated, learned: the Galerkin coefficient
+    ws_coef[0] = ws_mode != IBPM_WS_PREVIOUS && ws_mode != IBPM_WS_DIRECT ? cg_s_h[5] : 0.0;
     ws_coef[1] = ws_mode == IBPM_WS_LEARNED ? cg_s_h[6] : 0.0;
     if (last_cg_iters >= opt.cg_maxiter) cg_hit_maxiter = true;
+    if (ws_mode == IBPM_WS_DIRECT && err_h[1]) {
+        const int k = err_h[1];
+        err_h[1] = 0;
+        CK(cudaMemsetAsync(err + 1, 0, sizeof(int), st));
+        throw ApiError{IBPM_ERR_INVALID, "B is not positive definite (pivot " + std::to_string(k) + ")"};
+    }
     if (err_h[3]) {
         CK(cudaMemsetAsync(err + 2, 0, sizeof(int), st));
         throw ApiError{IBPM_ERR_NONFINITE, "non-finite residual in CG"};
@@ -1012,6 +1082,10 @@ void Engine<T>::step(const ibpm_step_params &sp) {
         }
         compute_bbox();
         check_region_error();
+        if (ws_mode == IBPM_WS_DIRECT) {
+            if (ws_since % ws_refresh == 0) direct_rebuild();
+            ++ws_since;
+        }
     }
     stage_release();
     q0_zero = false;
@@ -1023,6 +1097,7 @@ void Engine<T>::step(const ibpm_step_params &sp) {
         const int p = gc;
         if (!graph_exec[p]) {
             const int gc0 = gc, nc0 = nc;
+            const long long l0 = launches;  // the capture launches nothing
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             try {
                 step_body();
@@ -1033,12 +1108,14 @@ void Engine<T>::step(const ibpm_step_params &sp) {
                 (void)cudaGetLastError();
                 gc = gc0;
                 nc = nc0;
+                launches = l0;
                 throw;
             }
             CK(cudaStreamEndCapture(st, &graph[p]));
             CK(cudaGraphInstantiate(&graph_exec[p], graph[p], 0));
             gc = gc0;
             nc = nc0;
+            launches = l0;
         }
         CK(cudaGraphLaunch(graph_exec[p], st));
         launches += graph_launches[p];
@@ -1097,6 +1174,15 @@ void Engine<T>::step_body() {
         launch_ws_direction(Fbt, Fprev, np, ws_z, st);
         check_launch();
         if (ws_mode == IBPM_WS_PREVIOUS) {
+            cg(Fbt, Ftmp);
+        } else if (ws_mode == IBPM_WS_DIRECT) {
+            // x0 = B^-1 b with the inverse of this step's B (or, between rebuilds,
+            // of a recent step's); CG then checks x0 against its tolerance
+            const int nchunk = (n + 63) / 64;
+            binv_gemv_kernel<<<dim3(nchunk, nchunk), 256, 0, st>>>(Binv, Ftmp, part, n);
+            check_launch();
+            binv_reduce_kernel<<<1, 1024, 0, st>>>(part, nchunk, n, Fbt, fb, total, g.h, g.dt, 1);
+            check_launch();
             cg(Fbt, Ftmp);
         } else if (ws_mode == IBPM_WS_PROJECTED) {
             // Galerkin over the last ws_depth solutions, B applied to all in one batch
@@ -1292,8 +1378,21 @@ void Engine<T>::set_warm_start(ibpm_net *net, int mode, int depth) {
     CK(cudaSetDevice(device));
     if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
     if (mode != IBPM_WS_PREVIOUS && mode != IBPM_WS_LEARNED && mode != IBPM_WS_EXTRAPOLATED &&
-        mode != IBPM_WS_PROJECTED)
+        mode != IBPM_WS_PROJECTED && mode != IBPM_WS_DIRECT)
         throw ApiError{IBPM_ERR_INVALID, "unknown warm-start mode"};
+    if (mode == IBPM_WS_DIRECT) {
+        if (!std::is_same<T, double>::value)
+            throw ApiError{IBPM_ERR_INVALID, "the direct start needs the FP64 engine"};
+        if (depth < 1 || depth > (1 << 20)) throw ApiError{IBPM_ERR_INVALID, "the rebuild interval (depth) must be 1 .. 1048576"};
+        // all 2 np columns in one batch where about 16 GB of column work allows
+        const long long per_col = (2 * ng * L + nq + 2 * ng) * (long long)sizeof(T);
+        grow_batch_buffers((int)std::min<long long>(2 * np, std::max(1LL, (16LL << 30) / per_col)));
+        const int n = 2 * np;
+        if (!Binv) Binv = dalloc<double>((size_t)n * n);
+        if (!Bwork) Bwork = dalloc<double>((size_t)n * n);
+        ws_refresh = depth;
+        ws_since = 0;
+    }
     if (mode == IBPM_WS_PROJECTED) {
         if (depth < 1 || depth > 16) throw ApiError{IBPM_ERR_INVALID, "projection depth must be 1 .. 16"};
         grow_batch_buffers(depth);

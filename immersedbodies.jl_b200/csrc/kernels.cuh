@@ -762,35 +762,29 @@ static __global__ void binv_reduce_kernel(const double *__restrict__ part, int n
     }
 }
 
-// In-place Gauss-Jordan inversion of a symmetric positive definite matrix
-// (stands in for LinearAlgebra.inv at src/coupling.jl:190).  Step k, part 1:
-// save the pivot row/column.
-static __global__ void gj_save_kernel(const double *__restrict__ A, int n, int k, double *__restrict__ rowk,
-                               double *__restrict__ colk, int *err) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const double p = A[k + (long long)n * k];
-    if (t == 0 && !(p > 0.0)) atomicCAS(err, 0, k + 1);
-    rowk[t] = A[k + (long long)n * t] / p;
-    colk[t] = A[t + (long long)n * k];
-}
-// part 2: rank-1 update of every element
-static __global__ void gj_update_kernel(double *__restrict__ A, int n, int k, const double *__restrict__ rowk,
-                                 const double *__restrict__ colk) {
+// Gauss-Jordan inversion without pivoting of a positive definite matrix (stands
+// in for LinearAlgebra.inv at src/coupling.jl:190), one launch per step k from
+// S into D (ping-pong buffers, so no element is read after another thread
+// overwrote it): D = the step-k elimination of S, the pivot row scaled by 1/p,
+// the pivot column by -1/p and the pivot by 1/p.  A pivot <= 0 sets *err = k+1.
+static __global__ void gj_step_kernel(const double *__restrict__ S, double *__restrict__ D, int n, int k, int *err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= n) return;
-    const double p = colk[k];
+    const double p = S[k + (long long)n * k];
+    if (i == 0 && j == 0 && !(p > 0.0)) atomicCAS(err, 0, k + 1);
+    const double rk = S[k + (long long)n * j] / p;  // scaled pivot row
+    const double ck = S[i + (long long)n * k];      // pivot column
     double v;
     if (i == k && j == k)
         v = 1.0 / p;
     else if (i == k)
-        v = rowk[j];
+        v = rk;
     else if (j == k)
-        v = -colk[i] / p;
+        v = -ck / p;
     else
-        v = A[i + (long long)n * j] - colk[i] * rowk[j];
-    A[i + (long long)n * j] = v;
+        v = S[i + (long long)n * j] - ck * rk;
+    D[i + (long long)n * j] = v;
 }
 
 // Identity columns [c0, c0+nb) of a 2np-length basis, one per batch.

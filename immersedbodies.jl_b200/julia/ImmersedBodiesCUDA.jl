@@ -193,10 +193,12 @@ level_y_velocity(solver::GpuCnabSolver, level::Integer=1) =
     _level_field(solver, 2, level, (_base_n(solver)[1], _base_n(solver)[2] + 1))
 
 # CG initial guess for moving bodies: :previous (the reference's start), :extrapolated,
-# or :projected over the last `depth` solutions (1..16); plain CG then runs to the
-# configured tolerance.  (The learned mode needs a network made with ibpm_net_*.)
+# :projected over the last `depth` solutions (1..16), or :direct (B^-1 b with B
+# assembled and inverted on the GPU every `depth` steps, FP64 only); plain CG then
+# runs to the configured tolerance.  (The learned mode needs a network made with
+# ibpm_net_*.)
 function set_warm_start!(solver::GpuCnabSolver, mode::Symbol=:projected; depth::Integer=16)
-    m = Dict(:previous => 0, :extrapolated => 2, :projected => 3)[mode]
+    m = Dict(:previous => 0, :extrapolated => 2, :projected => 3, :direct => 4)[mode]
     _check(solver.handle, ccall((:ibpm_set_warm_start, libibpm), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32),
         solver.handle, m, C_NULL, depth))
     solver

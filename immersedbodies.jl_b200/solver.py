@@ -236,11 +236,13 @@ class GpuCnabSolver(AbstractSolver):
         """CG initial guess of this moving-body solver: "previous" (the reference's
         start from the previous F~b), "extrapolated" (Galerkin step along the last
         change F1 - F2), "learned" (then along a `WarmStartNet`'s correction; the
-        default when net is given) or "projected" (Galerkin over the last `depth`
-        solutions).  Keep the network alive while it is installed."""
+        default when net is given), "projected" (Galerkin over the last `depth`
+        solutions) or "direct" (B^-1 b, B assembled and inverted on the GPU every
+        `depth` steps; FP64 only).  Keep the network alive while it is installed."""
         mode = mode or ("learned" if net is not None else "previous")
         m = {"previous": _abi.IBPM_WS_PREVIOUS, "learned": _abi.IBPM_WS_LEARNED,
-             "extrapolated": _abi.IBPM_WS_EXTRAPOLATED, "projected": _abi.IBPM_WS_PROJECTED}[mode]
+             "extrapolated": _abi.IBPM_WS_EXTRAPOLATED, "projected": _abi.IBPM_WS_PROJECTED,
+             "direct": _abi.IBPM_WS_DIRECT}[mode]
         _abi.check(self.lib, self._h, self.lib.ibpm_set_warm_start(self._h, m, net.handle if net is not None else None,
                                                                     depth))
         self._warm_net = net

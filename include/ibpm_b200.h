@@ -256,13 +256,22 @@ const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed
  *                         (projection for successive right-hand sides); the history
  *                         restarts from the current solution when the mode or the
  *                         state is set
+ *   IBPM_WS_DIRECT        B^-1 b: B assembled for the step's body position from its
+ *                         2 npanel columns (batched applications, as the static-body
+ *                         B^-1 of src/coupling.jl:187-192) and inverted on the GPU,
+ *                         every `depth` (1 .. 1048576) steps, the first on the next
+ *                         step; between rebuilds the last inverse gives the guess.
+ *                         FP64 handles only; keeps a (2 npanel)^2 matrix and the
+ *                         column-batch work buffers (up to about 4 GB)
  * where the coefficients minimise the B-energy norm of the error over their
  * directions (Galerkin steps with B of the current step, applied in batched
- * passes; CG reuses B x0). */
+ * passes; CG reuses B x0).  CG then runs from the guess to its tolerance in
+ * every mode. */
 #define IBPM_WS_PREVIOUS 0
 #define IBPM_WS_LEARNED 1
 #define IBPM_WS_EXTRAPOLATED 2
 #define IBPM_WS_PROJECTED 3
+#define IBPM_WS_DIRECT 4
 int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t depth);
 /* The last step's warm-start features (10 x npanel floats), target (2 x
  * npanel: the converged F~b minus the extrapolated guess x_e) and, in the

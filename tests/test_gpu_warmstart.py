@@ -100,6 +100,42 @@ def test_every_start_reaches_the_same_forces(ib):
     assert iters["projected"][10:].mean() < iters["extrapolated"][10:].mean()
 
 
+def test_direct_start_matches_the_reference_start(ib):
+    """B assembled and inverted on the GPU each step (or every 4th): CG starts at
+    B^-1 b, so it needs no iterations on a rebuild step, and every start reaches
+    the forces of the reference's start to the CG tolerance.  Between rebuilds
+    the inverse of a few steps back gives a guess no worse than the reference's
+    (B moves with the body, so it saves only a few iterations)."""
+    runs = {}
+    for mode, depth in (("previous", 8), ("direct", 1), ("direct", 4)):
+        s = _plate(ib, 0.5)
+        if mode != "previous":
+            s.set_warm_start(None, mode=mode, depth=depth)
+        runs[(mode, depth)] = (_iters(s, 24), s.total_force().copy())
+        del s
+    it0, f0 = runs[("previous", 8)]
+    for key in (("direct", 1), ("direct", 4)):
+        it, f = runs[key]
+        assert np.abs(f - f0).max() <= 1e-6 * np.abs(f0).max(), key
+    assert runs[("direct", 1)][0].max() <= 1
+    it4 = runs[("direct", 4)][0]
+    assert it4[::4].max() <= 1  # rebuild steps
+    assert it4[8:].mean() <= 1.05 * it0[8:].mean()
+
+
+def test_direct_start_inverts_the_current_B(ib):
+    """After a step the direct start's inverse is the inverse of B at the step's
+    body position, B assembled here column by column through diag_apply_B."""
+    s = _plate(ib, 0.5)
+    s.set_warm_start(None, mode="direct", depth=1)
+    for _ in range(3):
+        s.advance_()
+    n = 2 * s.state.prob.bodies.npanel
+    B = np.stack([s.diag_apply_B(np.eye(n)[k]) for k in range(n)], axis=1)
+    Binv = s.diag_binv()
+    assert np.abs(Binv @ B - np.eye(n)).max() <= 1e-8
+
+
 def test_learned_warm_start_on_a_held_out_frequency(ib, capsys):
     """Trained on samples of k = 0.3 and 0.7, run at k = 0.5.  The learned start
     includes the extrapolation step, so it must use fewer CG iterations than the
@@ -152,3 +188,9 @@ def test_warm_start_errors(ib):
     wrong = ib.WarmStartNet(cin=4, width=8, layers=2)
     with pytest.raises(ib._abi.IbpmError, match="10 feature channels"):
         s.set_warm_start(wrong)
+    with pytest.raises(ib._abi.IbpmError, match="rebuild interval"):
+        s.set_warm_start(None, mode="direct", depth=0)
+    prob = ib.configs.pitching_plate(0.5, h=0.04, n=128, nlevel=3, npts=26, dt=0.004)
+    s32 = ib.GpuCnabSolver(ib.State(prob), cg=CG, precision="fp32")
+    with pytest.raises(ib._abi.IbpmError, match="FP64 engine"):
+        s32.set_warm_start(None, mode="direct")
