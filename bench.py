@@ -258,6 +258,42 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
             "steps_per_s_vs_previous": {m: out[m]["steps_per_s"] / base["steps_per_s"] for m in out}}
 
 
+def direct_start_run(ib, device: int, steps: int, warmup: int):
+    """The direct CG start alone (B assembled and inverted on the GPU every step)
+    on the 512^2 x 4-level pitching plate at k = 0.55: `warmup` steps, then
+    `steps` steps timed with CUDA events on the solver's stream, the last of them
+    inside the NVTX range "direct_step" (the range a kernel-launch list selects)."""
+    import torch
+
+    s = ib.GpuCnabSolver(ib.State(ib.configs.pitching_plate(0.55)), cg=dict(reltol=0.0, abstol=1e-10, maxiter=5000),
+                         device=device)
+    s.set_warm_start(None, mode="direct", depth=1)
+    for _ in range(warmup):
+        s.advance_()
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    it = []
+    torch.cuda.synchronize()
+    l0 = s.kernel_launches()
+    e0.record(stream)
+    for k in range(steps):
+        if k == steps - 1:
+            torch.cuda.nvtx.range_push("direct_step")
+        s.advance_()
+        it.append(s.info().last_cg_iters)
+        if k == steps - 1:
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"metric": "moving-body steps/s, direct CG start", "value": 1000.0 / ms, "unit": "steps/s",
+            "ms_per_step": ms, "steps": steps, "warmup": warmup, "cg_iterations_mean": float(np.mean(it)),
+            "gpu_launches_per_step": (s.kernel_launches() - l0) / steps,
+            "config": {"workload": "pitching_plate_512: 512x512 cells x 4 levels, 101-point plate, Re 500, dt 0.002, "
+                                   "k = 0.55; CG to |r| <= 1e-10", "precision": "fp64"}}
+
+
 def ensemble_report(ib, device: int, seed: int = 2026, n: int = 128, steps: int = 10):
     """Case-steps/s of n independent FP32 cases (finest grids of {256, 384, 512} x
     256 cells at h 0.01, 3 levels, seeded cylinders or plates, Re ~ U[50, 300],
@@ -323,10 +359,18 @@ def main():
     ap.add_argument("--no-chosen", action="store_true", help="skip the mixed-precision engine")
     ap.add_argument("--no-learned", action="store_true", help="skip the moving-body CG warm-start comparison")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 128-case ensemble measurement")
+    ap.add_argument("--direct-start-only", action="store_true",
+                    help="time only the moving-body direct CG start (one JSON line) and exit")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.direct_start_only:
+        ib = load_package()
+        line = direct_start_run(ib, local, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
 
     import torch
 

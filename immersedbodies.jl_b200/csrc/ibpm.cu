@@ -814,9 +814,8 @@ void Engine<T>::build_Binv() {
 
 // B of the current body position into Binv, kbatch columns per batched
 // application, then inverted by Gauss-Jordan elimination without pivoting
-// between Binv and Bwork (B is positive definite; its multi-level
-// discretisation leaves it symmetric only to about 1e-6 relative); a pivot
-// <= 0 sets err[1].
+// between Binv and Bwork (the symmetric part of B is positive definite; with
+// nested levels B itself is not exactly symmetric); a pivot <= 0 sets err[1].
 template <class T>
 void Engine<T>::assemble_invert_B() {
     const int n = 2 * np;

@@ -262,7 +262,7 @@ const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed
  *                         every `depth` (1 .. 1048576) steps, the first on the next
  *                         step; between rebuilds the last inverse gives the guess.
  *                         FP64 handles only; keeps a (2 npanel)^2 matrix and the
- *                         column-batch work buffers (up to about 4 GB)
+ *                         column-batch work buffers (up to about 16 GB)
  * where the coefficients minimise the B-energy norm of the error over their
  * directions (Galerkin steps with B of the current step, applied in batched
  * passes; CG reuses B x0).  CG then runs from the guess to its tolerance in
