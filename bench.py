@@ -191,8 +191,9 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
     pitching and plunging plate, 101 points, Re 500, dt 0.002, CG to an absolute
     residual of 1e-10) at a held-out reduced frequency k = 0.55, with the
     reference's start (the previous solution), the extrapolated start, the
-    learned start, the projection onto the last 16 solutions and the direct start
-    (B assembled and inverted on the GPU every step, or every 8th); the network is
+    learned start, the projection onto the last 16 solutions, the direct start
+    (B assembled and inverted on the GPU every step, or every 8th) and CG
+    preconditioned by that inverse rebuilt every 8th or 32nd step; the network is
     trained on samples of k = 0.25, 0.45, 0.65 and 0.85 generated by the solver
     (after a 60-step start-up).  Every run takes the same steps, so their final
     forces differ only by the CG tolerance."""
@@ -214,7 +215,8 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
     t_train = time.perf_counter() - t0
     out, forces = {}, {}
     runs = (("previous", "previous", 16), ("extrapolated", "extrapolated", 16), ("learned", "learned", 16),
-            ("projected", "projected", 16), ("direct", "direct", 1), ("direct_every_8", "direct", 8))
+            ("projected", "projected", 16), ("direct", "direct", 1), ("direct_every_8", "direct", 8),
+            ("preconditioned_every_8", "preconditioned", 8), ("preconditioned_every_32", "preconditioned", 32))
     for label, mode, depth in runs:
         s = make(0.55)
         if mode != "previous":

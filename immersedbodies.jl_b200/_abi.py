@@ -102,7 +102,8 @@ EXPORTS = {
     "ibpm_lap_inv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ibpm_noalloc_last_error": (C.c_char_p, []),
 }
-IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED, IBPM_WS_PROJECTED, IBPM_WS_DIRECT = 0, 1, 2, 3, 4
+(IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED, IBPM_WS_PROJECTED, IBPM_WS_DIRECT,
+ IBPM_WS_PRECONDITIONED) = 0, 1, 2, 3, 4, 5
 KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5}
 
 _lib = None

@@ -188,8 +188,10 @@ struct Engine final : ibpm_handle {
     ibpm_net *ws = nullptr;
     int ws_mode = IBPM_WS_PREVIOUS;
     int ws_depth = 0;                       // previous solutions kept for IBPM_WS_PROJECTED
-    // IBPM_WS_DIRECT: B^-1 of the body position, rebuilt every ws_refresh steps
-    // (ws_since counts the steps since the last rebuild) by its own graph
+    // IBPM_WS_DIRECT / IBPM_WS_PRECONDITIONED: B^-1 of the body position, rebuilt
+    // every ws_refresh steps (ws_since counts the steps since the last rebuild) by
+    // its own graph
+    bool uses_binv_start() const { return ws_mode == IBPM_WS_DIRECT || ws_mode == IBPM_WS_PRECONDITIONED; }
     int ws_refresh = 1;
     long long ws_since = 0;
     cudaGraph_t binv_graph = nullptr;
@@ -210,7 +212,7 @@ struct Engine final : ibpm_handle {
     T *Gw = nullptr, *psiw = nullptr, *qw = nullptr;  // batch work (K columns)
     double *fcol = nullptr;
     double *Binv = nullptr, *Bwork = nullptr;  // B^-1 and the Gauss-Jordan ping-pong buffer
-    double *cg_u = nullptr, *cg_r = nullptr, *cg_c = nullptr, *cg_s = nullptr, *cg_s_h = nullptr;
+    double *cg_u = nullptr, *cg_r = nullptr, *cg_c = nullptr, *cg_z = nullptr, *cg_s = nullptr, *cg_s_h = nullptr;
     int *err = nullptr, *err_h = nullptr;
     int last_cg_iters = 0;
     double last_cg_res = 0.0, first_cg_res = 0.0, ws_coef[2] = {0.0, 0.0};
@@ -604,7 +606,7 @@ struct Engine final : ibpm_handle {
     void assemble_invert_B();
     void direct_rebuild();
     int batch_width() const;
-    void cg(double *x, const double *b, bool have_bx = false);
+    void cg(double *x, const double *b, bool have_bx = false, bool precond = false);
     void cg_collect();
     int *cg_it = nullptr;
     bool cg_pending = false, cg_hit_maxiter = false;
@@ -749,9 +751,10 @@ void Engine<T>::setup() {
     qw = dalloc<T>(nq * kbatch);
     fcol = dalloc<double>(2 * (size_t)np * kbatch);
     cg_u = dalloc<double>(2 * np);
+    cg_z = dalloc<double>(2 * np);
     cg_r = dalloc<double>(2 * np);
     cg_c = dalloc<double>(2 * np);
-    cg_s = dalloc<double>(8);
+    cg_s = dalloc<double>(16);
     cg_it = dalloc<int>(4);
     CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
 
@@ -867,6 +870,7 @@ void Engine<T>::direct_rebuild() {
 namespace {
 // Device-resident CG state: s[0] = ||r||, s[1] = previous ||r||, s[2] = tol,
 // s[3] = 1 while iterating; it[0] = iterations; err[2] = 1 on a non-finite residual.
+// Preconditioned (pre = 1): s[8] = rho = r . z of the last direction, z = M r in z.
 struct CgArgs {
     int n;
     double *x, *r, *u, *c;
@@ -875,6 +879,8 @@ struct CgArgs {
     int *it, *err;
     int maxiter;
     double reltol, abstol;
+    int pre;
+    double *z;
 };
 
 __device__ __forceinline__ double cg_block_sum(double v, double *red) {
@@ -912,6 +918,7 @@ __global__ void cg_init_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h
         a.s[2] = tol;
         a.s[3] = cont;
         a.s[4] = res;  // initial residual, for reports
+        a.s[8] = 1.0;  // rho before the first direction (u = 0 makes it immaterial)
         a.it[0] = 0;
         if (use_h) cudaGraphSetConditional(h, cont ? 1u : 0u);
     }
@@ -924,14 +931,39 @@ __global__ void cg_dir_kernel(CgArgs a) {
         a.u[k] = a.r[k] + beta * a.u[k];
 }
 
-// alpha = ||r||^2 / (u . c); x += alpha u; r -= alpha c; new residual and condition
+// Preconditioned direction (one block): z = M r from binv_gemv_kernel's chunk
+// partials, rho = r . z, u = z + (rho / rho_prev) u -- IterativeSolvers' cg
+// iteration with a left preconditioner (rho = r . (Pl \ r)); M = B^-1 of a
+// recent step.
+__global__ void pcg_dir_kernel(CgArgs a, const double *__restrict__ part, int nchunk) {
+    __shared__ double red[32];
+    __shared__ double beta_s;
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < a.n; k += blockDim.x) {
+        double z = 0.0;
+        for (int c = 0; c < nchunk; ++c) z += part[(long long)c * a.n + k];
+        a.z[k] = z;
+        acc += a.r[k] * z;
+    }
+    const double rho = cg_block_sum(acc, red);
+    if (threadIdx.x == 0) {
+        beta_s = rho / a.s[8];
+        a.s[8] = rho;
+    }
+    __syncthreads();
+    const double beta = beta_s;
+    for (int k = threadIdx.x; k < a.n; k += blockDim.x) a.u[k] = a.z[k] + beta * a.u[k];
+}
+
+// alpha = rho / (u . c), rho = ||r||^2 (plain) or r . z (preconditioned);
+// x += alpha u; r -= alpha c; new residual and condition
 __global__ void cg_update_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h) {
     __shared__ double red[32];
     __shared__ double alpha_s;
     double acc = 0.0;
     for (int k = threadIdx.x; k < a.n; k += blockDim.x) acc += a.u[k] * a.c[k];
     const double uc = cg_block_sum(acc, red);
-    if (threadIdx.x == 0) alpha_s = a.s[0] * a.s[0] / uc;
+    if (threadIdx.x == 0) alpha_s = (a.pre ? a.s[8] : a.s[0] * a.s[0]) / uc;
     __syncthreads();
     const double alpha = alpha_s;
     double rr = 0.0;
@@ -961,13 +993,29 @@ __global__ void cg_update_kernel(CgArgs a, cudaGraphConditionalHandle h, int use
 
 // IterativeSolvers.jl cg! as called at src/coupling.jl:198-201: plain CG from
 // the initial guess x; stops when ||r|| <= max(reltol ||r0||, abstol) or after
-// maxiter iterations.  All scalars live on the device.  Inside a stream
+// maxiter iterations.  precond: the same iteration with the left
+// preconditioner Pl = B of a recent step, applied as z = Binv r (the reference
+// passes no Pl; the stopping rule on ||r|| is unchanged).  All scalars live on
+// the device.  Inside a stream
 // capture the loop is a graph WHILE node whose condition the update kernel
 // sets; otherwise the host reads the condition after every iteration.
 template <class T>
-void Engine<T>::cg(double *x, const double *b, bool have_bx) {
+void Engine<T>::cg(double *x, const double *b, bool have_bx, bool precond) {
     const int n = 2 * np;
-    CgArgs a{n, x, cg_r, cg_u, cg_c, b, cg_s, cg_it, err, opt.cg_maxiter, opt.cg_reltol, opt.cg_abstol};
+    const int nchunk = (n + 63) / 64;
+    CgArgs a{n, x, cg_r, cg_u, cg_c, b, cg_s, cg_it, err, opt.cg_maxiter, opt.cg_reltol, opt.cg_abstol, precond ? 1 : 0,
+             cg_z};
+    // the direction: plain, or preconditioned by Binv (z = Binv r)
+    auto direction = [&]() {
+        if (precond) {
+            binv_gemv_kernel<<<dim3(nchunk, nchunk), 256, 0, st>>>(Binv, cg_r, part, n);
+            check_launch();
+            pcg_dir_kernel<<<1, 256, 0, st>>>(a, part, nchunk);
+        } else {
+            cg_dir_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
+        }
+        check_launch();
+    };
     if (!have_bx) apply_B(x, cg_c, n, 1);  // else cg_c already holds B x
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
@@ -995,8 +1043,7 @@ void Engine<T>::cg(double *x, const double *b, bool have_bx) {
         st = st_side;
         try {
             CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-            cg_dir_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
-            check_launch();
+            direction();
             apply_B(cg_u, cg_c, n, 1);
             cg_update_kernel<<<1, 256, 0, st>>>(a, hnd, 1);
             check_launch();
@@ -1017,8 +1064,7 @@ void Engine<T>::cg(double *x, const double *b, bool have_bx) {
         CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (cg_s_h[3] == 0.0) break;
-        cg_dir_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
-        check_launch();
+        direction();
         apply_B(cg_u, cg_c, n, 1);
         cg_update_kernel<<<1, 256, 0, st>>>(a, 0, 0);
         check_launch();
@@ -1032,17 +1078,17 @@ void Engine<T>::cg_collect() {
     CK(cudaMemcpyAsync(cg_s_h, cg_s, sizeof(double) * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_h + 2, cg_it, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_h + 3, err + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (ws_mode == IBPM_WS_DIRECT) CK(cudaMemcpyAsync(err_h + 1, err + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (uses_binv_start()) CK(cudaMemcpyAsync(err_h + 1, err + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     cg_pending = false;
     last_cg_iters = err_h[2];
     last_cg_res = cg_s_h[0];
     first_cg_res = cg_s_h[4];
     // projected: directions kept; extrapolated, learned: the Galerkin coefficient
-    ws_coef[0] = ws_mode != IBPM_WS_PREVIOUS && ws_mode != IBPM_WS_DIRECT ? cg_s_h[5] : 0.0;
+    ws_coef[0] = ws_mode != IBPM_WS_PREVIOUS && !uses_binv_start() ? cg_s_h[5] : 0.0;
     ws_coef[1] = ws_mode == IBPM_WS_LEARNED ? cg_s_h[6] : 0.0;
     if (last_cg_iters >= opt.cg_maxiter) cg_hit_maxiter = true;
-    if (ws_mode == IBPM_WS_DIRECT && err_h[1]) {
+    if (uses_binv_start() && err_h[1]) {
         const int k = err_h[1];
         err_h[1] = 0;
         CK(cudaMemsetAsync(err + 1, 0, sizeof(int), st));
@@ -1081,7 +1127,7 @@ void Engine<T>::step(const ibpm_step_params &sp) {
         }
         compute_bbox();
         check_region_error();
-        if (ws_mode == IBPM_WS_DIRECT) {
+        if (uses_binv_start()) {
             if (ws_since % ws_refresh == 0) direct_rebuild();
             ++ws_since;
         }
@@ -1174,15 +1220,16 @@ void Engine<T>::step_body() {
         check_launch();
         if (ws_mode == IBPM_WS_PREVIOUS) {
             cg(Fbt, Ftmp);
-        } else if (ws_mode == IBPM_WS_DIRECT) {
+        } else if (uses_binv_start()) {
             // x0 = B^-1 b with the inverse of this step's B (or, between rebuilds,
-            // of a recent step's); CG then checks x0 against its tolerance
+            // of a recent step's); CG then runs from x0, preconditioned by the
+            // same inverse in IBPM_WS_PRECONDITIONED
             const int nchunk = (n + 63) / 64;
             binv_gemv_kernel<<<dim3(nchunk, nchunk), 256, 0, st>>>(Binv, Ftmp, part, n);
             check_launch();
             binv_reduce_kernel<<<1, 1024, 0, st>>>(part, nchunk, n, Fbt, fb, total, g.h, g.dt, 1);
             check_launch();
-            cg(Fbt, Ftmp);
+            cg(Fbt, Ftmp, false, ws_mode == IBPM_WS_PRECONDITIONED);
         } else if (ws_mode == IBPM_WS_PROJECTED) {
             // Galerkin over the last ws_depth solutions, B applied to all in one batch
             apply_B(ws_hist, ws_bhist, 2 * np, ws_depth);
@@ -1377,11 +1424,11 @@ void Engine<T>::set_warm_start(ibpm_net *net, int mode, int depth) {
     CK(cudaSetDevice(device));
     if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
     if (mode != IBPM_WS_PREVIOUS && mode != IBPM_WS_LEARNED && mode != IBPM_WS_EXTRAPOLATED &&
-        mode != IBPM_WS_PROJECTED && mode != IBPM_WS_DIRECT)
+        mode != IBPM_WS_PROJECTED && mode != IBPM_WS_DIRECT && mode != IBPM_WS_PRECONDITIONED)
         throw ApiError{IBPM_ERR_INVALID, "unknown warm-start mode"};
-    if (mode == IBPM_WS_DIRECT) {
+    if (mode == IBPM_WS_DIRECT || mode == IBPM_WS_PRECONDITIONED) {
         if (!std::is_same<T, double>::value)
-            throw ApiError{IBPM_ERR_INVALID, "the direct start needs the FP64 engine"};
+            throw ApiError{IBPM_ERR_INVALID, "the direct and preconditioned starts need the FP64 engine"};
         if (depth < 1 || depth > (1 << 20)) throw ApiError{IBPM_ERR_INVALID, "the rebuild interval (depth) must be 1 .. 1048576"};
         // all 2 np columns in one batch where about 16 GB of column work allows
         const long long per_col = (2 * ng * L + nq + 2 * ng) * (long long)sizeof(T);

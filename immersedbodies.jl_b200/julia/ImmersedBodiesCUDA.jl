@@ -195,10 +195,11 @@ level_y_velocity(solver::GpuCnabSolver, level::Integer=1) =
 # CG initial guess for moving bodies: :previous (the reference's start), :extrapolated,
 # :projected over the last `depth` solutions (1..16), or :direct (B^-1 b with B
 # assembled and inverted on the GPU every `depth` steps, FP64 only); plain CG then
-# runs to the configured tolerance.  (The learned mode needs a network made with
-# ibpm_net_*.)
+# runs to the configured tolerance.  :preconditioned is :direct with CG
+# preconditioned by that inverse (not the reference's iteration; same stopping
+# rule).  (The learned mode needs a network made with ibpm_net_*.)
 function set_warm_start!(solver::GpuCnabSolver, mode::Symbol=:projected; depth::Integer=16)
-    m = Dict(:previous => 0, :extrapolated => 2, :projected => 3, :direct => 4)[mode]
+    m = Dict(:previous => 0, :extrapolated => 2, :projected => 3, :direct => 4, :preconditioned => 5)[mode]
     _check(solver.handle, ccall((:ibpm_set_warm_start, libibpm), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32),
         solver.handle, m, C_NULL, depth))
     solver

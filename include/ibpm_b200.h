@@ -263,6 +263,11 @@ const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed
  *                         step; between rebuilds the last inverse gives the guess.
  *                         FP64 handles only; keeps a (2 npanel)^2 matrix and the
  *                         column-batch work buffers (up to about 16 GB)
+ *   IBPM_WS_PRECONDITIONED  as IBPM_WS_DIRECT, and CG is preconditioned by the same
+ *                         inverse (z = B_k^-1 r, B_k of the last rebuild): between
+ *                         rebuilds CG needs a few iterations instead of hundreds.
+ *                         Not the reference's iteration (it passes no
+ *                         preconditioner); the stopping rule on ||r|| is the same
  * where the coefficients minimise the B-energy norm of the error over their
  * directions (Galerkin steps with B of the current step, applied in batched
  * passes; CG reuses B x0).  CG then runs from the guess to its tolerance in
@@ -272,6 +277,7 @@ const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed
 #define IBPM_WS_EXTRAPOLATED 2
 #define IBPM_WS_PROJECTED 3
 #define IBPM_WS_DIRECT 4
+#define IBPM_WS_PRECONDITIONED 5
 int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t depth);
 /* The last step's warm-start features (10 x npanel floats), target (2 x
  * npanel: the converged F~b minus the extrapolated guess x_e) and, in the

@@ -123,6 +123,23 @@ def test_direct_start_matches_the_reference_start(ib):
     assert it4[8:].mean() <= 1.05 * it0[8:].mean()
 
 
+def test_preconditioned_cg_with_a_periodic_inverse(ib):
+    """CG preconditioned by B^-1 of the last rebuild (every 8th step): a few
+    iterations between rebuilds, and the forces of the reference's unpreconditioned
+    CG to its tolerance."""
+    runs = {}
+    for mode in ("previous", "preconditioned"):
+        s = _plate(ib, 0.5)
+        if mode != "previous":
+            s.set_warm_start(None, mode=mode, depth=8)
+        runs[mode] = (_iters(s, 24), s.total_force().copy())
+        del s
+    (it0, f0), (it, f) = runs["previous"], runs["preconditioned"]
+    assert np.abs(f - f0).max() <= 1e-6 * np.abs(f0).max()
+    assert it[::8].max() <= 1  # rebuild steps start at B^-1 b of their own B
+    assert it.max() <= 12 and it.mean() <= 0.1 * it0.mean(), (it, it0.mean())
+
+
 def test_direct_start_inverts_the_current_B(ib):
     """After a step the direct start's inverse is the inverse of B at the step's
     body position, B assembled here column by column through diag_apply_B."""
