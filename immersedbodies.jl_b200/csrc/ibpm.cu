@@ -31,6 +31,7 @@ using namespace ibpm;
 namespace {
 
 constexpr int kNG = 2;  // FFT groups (line pairs) per block
+constexpr int kNGWide = 4, kWideBatch = 16;  // Y-pass groups per block for launches over >= kWideBatch fields
 
 thread_local std::string g_create_error;
 
@@ -371,9 +372,30 @@ struct Engine final : ibpm_handle {
     template <class D>
     void ypass_t(const PlanT<typename D::Real> &pl, const typename D::Real *in, typename D::Real *out, long long bs,
                  int nbatch, Mult m) {
-        const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nbatch);
-        const size_t sm = pass_smem<D>(pl.M, kNG, kNG);
-        ypass_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(in, out, bs, nx - 1, pl, m);
+        if constexpr (D::MC > 0) {
+            if (nbatch >= kWideBatch) {
+                ypass_launch<D, kNGWide>(pl, in, out, bs, nbatch, m);
+                return;
+            }
+        }
+        ypass_launch<D, kNG>(pl, in, out, bs, nbatch, m);
+    }
+    // Y pass with NGY line pairs (2 NGY columns) per block.  Launches over many
+    // fields (the B assembly) have waves to spare, and wider blocks read longer
+    // segments of each row.
+    template <class D, int NGY>
+    void ypass_launch(const PlanT<typename D::Real> &pl, const typename D::Real *in, typename D::Real *out, long long bs,
+                      int nbatch, Mult m) {
+        const dim3 grid((nx - 1 + 2 * NGY - 1) / (2 * NGY), nbatch);
+        const size_t sm = pass_smem<D>(pl.M, NGY, NGY);
+        if (sm > 48 * 1024) {
+            static bool attr = false;  // one M per compile-time transform, so one size
+            if (!attr) {
+                CK(cudaFuncSetAttribute(ypass_kernel<D, NGY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                attr = true;
+            }
+        }
+        ypass_kernel<D, NGY><<<grid, NGY * D::TPF, sm, st>>>(in, out, bs, nx - 1, pl, m);
     }
     template <class R = T>
     void ypass(const R *in, R *out, long long bs, int nbatch, Mult m) {
@@ -828,13 +850,15 @@ void Engine<T>::assemble_invert_B() {
         check_launch();
         apply_B(fcol, Binv + (size_t)c0 * n, n, nb);
     }
-    for (int k = 0; k < n; ++k) {
-        // n = 2 np is even: the last step writes Binv
-        const double *src = (k & 1) ? Bwork : Binv;
-        double *dst = (k & 1) ? Binv : Bwork;
-        gj_step_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(src, dst, n, k, err + 1);
+    // n = 2 np is even: n / 2 two-step launches; after an odd count the result is in Bwork
+    int m = 0;
+    for (int k = 0; k < n; k += 2, ++m) {
+        const double *src = (m & 1) ? Bwork : Binv;
+        double *dst = (m & 1) ? Binv : Bwork;
+        gj_step2_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(src, dst, n, k, err + 1);
         check_launch();
     }
+    if (m & 1) CK(cudaMemcpyAsync(Binv, Bwork, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, st));
 }
 
 // IBPM_WS_DIRECT's rebuild of B^-1 for the body position of this step, as a graph

@@ -787,6 +787,43 @@ static __global__ void gj_step_kernel(const double *__restrict__ S, double *__re
     D[i + (long long)n * j] = v;
 }
 
+// Element (a, b) after Gauss-Jordan step k of S: the expression of gj_step_kernel.
+__device__ __forceinline__ double gj_elem(const double *__restrict__ S, int n, int k, int a, int b) {
+    const double p = S[k + (long long)n * k];
+    if (a == k && b == k) return 1.0 / p;
+    if (a == k) return S[k + (long long)n * b] / p;
+    if (b == k) return -S[a + (long long)n * k] / p;
+    return S[a + (long long)n * b] - S[a + (long long)n * k] * (S[k + (long long)n * b] / p);
+}
+// Steps k and k+1 in one launch: the step-(k+1) expression applied to the
+// step-k elements, each formed as gj_step_kernel forms it (same results bit for
+// bit, half the launches).  A pivot <= 0 sets *err to its step + 1.
+static __global__ void gj_step2_kernel(const double *__restrict__ S, double *__restrict__ D, int n, int k, int *err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= n) return;
+    const int k1 = k + 1;
+    const double q = gj_elem(S, n, k, k1, k1);
+    if (i == 0 && j == 0) {
+        if (!(S[k + (long long)n * k] > 0.0))
+            atomicCAS(err, 0, k + 1);
+        else if (!(q > 0.0))
+            atomicCAS(err, 0, k1 + 1);
+    }
+    const double rk = gj_elem(S, n, k, k1, j) / q;
+    const double ck = gj_elem(S, n, k, i, k1);
+    double v;
+    if (i == k1 && j == k1)
+        v = 1.0 / q;
+    else if (i == k1)
+        v = rk;
+    else if (j == k1)
+        v = -ck / q;
+    else
+        v = gj_elem(S, n, k, i, j) - ck * rk;
+    D[i + (long long)n * j] = v;
+}
+
 // Identity columns [c0, c0+nb) of a 2np-length basis, one per batch.
 static __global__ void unit_columns_kernel(double *__restrict__ f, int n, int c0, int nb) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
