@@ -763,31 +763,9 @@ static __global__ void binv_reduce_kernel(const double *__restrict__ part, int n
 }
 
 // Gauss-Jordan inversion without pivoting of a positive definite matrix (stands
-// in for LinearAlgebra.inv at src/coupling.jl:190), one launch per step k from
-// S into D (ping-pong buffers, so no element is read after another thread
-// overwrote it): D = the step-k elimination of S, the pivot row scaled by 1/p,
-// the pivot column by -1/p and the pivot by 1/p.  A pivot <= 0 sets *err = k+1.
-static __global__ void gj_step_kernel(const double *__restrict__ S, double *__restrict__ D, int n, int k, int *err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (i >= n) return;
-    const double p = S[k + (long long)n * k];
-    if (i == 0 && j == 0 && !(p > 0.0)) atomicCAS(err, 0, k + 1);
-    const double rk = S[k + (long long)n * j] / p;  // scaled pivot row
-    const double ck = S[i + (long long)n * k];      // pivot column
-    double v;
-    if (i == k && j == k)
-        v = 1.0 / p;
-    else if (i == k)
-        v = rk;
-    else if (j == k)
-        v = -ck / p;
-    else
-        v = S[i + (long long)n * j] - ck * rk;
-    D[i + (long long)n * j] = v;
-}
-
-// Element (a, b) after Gauss-Jordan step k of S: the expression of gj_step_kernel.
+// in for LinearAlgebra.inv at src/coupling.jl:190).  Element (a, b) after step k
+// of S: the pivot row scaled by 1/p, the pivot column by -1/p, the pivot by 1/p,
+// every other element S[a,b] - S[a,k] (S[k,b] / p).
 __device__ __forceinline__ double gj_elem(const double *__restrict__ S, int n, int k, int a, int b) {
     const double p = S[k + (long long)n * k];
     if (a == k && b == k) return 1.0 / p;
@@ -795,9 +773,10 @@ __device__ __forceinline__ double gj_elem(const double *__restrict__ S, int n, i
     if (b == k) return -S[a + (long long)n * k] / p;
     return S[a + (long long)n * b] - S[a + (long long)n * k] * (S[k + (long long)n * b] / p);
 }
-// Steps k and k+1 in one launch: the step-(k+1) expression applied to the
-// step-k elements, each formed as gj_step_kernel forms it (same results bit for
-// bit, half the launches).  A pivot <= 0 sets *err to its step + 1.
+// Steps k and k+1 in one launch, from S into D (ping-pong buffers, so no element
+// is read after another thread overwrote it): the step-(k+1) expression applied
+// to the step-k elements gj_elem forms, the same values bit for bit as two
+// one-step launches.  A pivot <= 0 sets *err to its step + 1.
 static __global__ void gj_step2_kernel(const double *__restrict__ S, double *__restrict__ D, int n, int k, int *err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
