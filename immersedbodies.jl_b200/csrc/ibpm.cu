@@ -595,7 +595,7 @@ struct Engine final : ibpm_handle {
     void set_state(const ibpm_state_view *s) override;
     void get_field(int field, int level, double *out) override;
     double *field_d = nullptr;  // one level of an output field
-        void set_warm_start(ibpm_net *net, int mode, int depth) override;
+    void set_warm_start(ibpm_net *net, int mode, int depth) override;
     void warm_start_sample(float *features, float *target, float *prediction) override;
     void get_state(ibpm_state_view *s) override;
     bool advance(int64_t nsteps, const ibpm_step_params *params) override;

@@ -33,6 +33,19 @@ def test_library_exports_all_declared(ib):
     assert set(declared_functions()) <= exported
 
 
+def test_header_constants_match_the_python_mirror(ib):
+    """Every integer #define of the header that the ctypes mirror also names has
+    the same value there (modes, precisions, fields, error codes)."""
+    from importlib import import_module
+
+    abi = import_module(ib.__name__ + "._abi")
+    defines = dict((k, int(v)) for k, v in re.findall(r"#define\s+(IBPM_\w+)\s+\(?(-?\d+)\)?", open(HEADER).read()))
+    shared = [k for k in defines if hasattr(abi, k)]
+    assert {"IBPM_WS_PREVIOUS", "IBPM_WS_DIRECT", "IBPM_WS_PRECONDITIONED", "IBPM_FP64"} <= set(shared), shared
+    for k in shared:
+        assert getattr(abi, k) == defines[k], k
+
+
 def test_create_without_gpu_fails_loudly(ib):
     """With no CUDA device the library refuses to create a solver (no CPU fallback)."""
     import torch

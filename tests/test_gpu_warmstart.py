@@ -140,6 +140,25 @@ def test_preconditioned_cg_with_a_periodic_inverse(ib):
     assert it.max() <= 12 and it.mean() <= 0.1 * it0.mean(), (it, it0.mean())
 
 
+def test_direct_and_preconditioned_eager_match_graphs(ib):
+    """With kernel profiling on, steps run eagerly: the B^-1 rebuild without its
+    graph and CG as a host loop.  Both modes give the graph path's iteration
+    counts and forces."""
+    out = {}
+    for mode in ("direct", "preconditioned"):
+        for eager in (False, True):
+            s = _plate(ib, 0.5)
+            s.set_warm_start(None, mode=mode, depth=4)
+            if eager:
+                s.profile(True)
+            out[(mode, eager)] = (_iters(s, 10), s.total_force().copy())
+            del s
+    for mode in ("direct", "preconditioned"):
+        (ig, fg), (ie, fe) = out[(mode, False)], out[(mode, True)]
+        assert np.array_equal(ig, ie), (mode, ig, ie)
+        assert np.abs(fe - fg).max() <= 1e-13 * np.abs(fg).max(), mode
+
+
 def test_direct_start_inverts_the_current_B(ib):
     """After a step the direct start's inverse is the inverse of B at the step's
     body position, B assembled here column by column through diag_apply_B."""
