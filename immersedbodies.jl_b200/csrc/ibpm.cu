@@ -347,24 +347,25 @@ struct Engine final : ibpm_handle {
     // Dispatch on the transform length: compile-time transforms for
     // M in {256, 384, 512, 1024}, the runtime mixed-radix one otherwise.
     template <class D, class In, class Out>
-    void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch) {
+    void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch, const int *rows) {
         const int pairs = (ny - 1 + 1) / 2;
         const dim3 grid((pairs + kNG - 1) / kNG, nbatch);
         const size_t sm = pass_smem<D>(pl.M, kNG, kNG);
-        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, pl, ny - 1);
+        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, pl, ny - 1, rows);
     }
     // X pass with transforms of element type R (the engine's T, or double for
     // the FP32 engine's FP64 level-1 solve); In/Out convert at the boundary.
+    // rows: see xpass_kernel (null: every row).
     template <class R = T, class In, class Out>
-    void xpass(In in, Out out, int nbatch) {
+    void xpass(In in, Out out, int nbatch, const int *rows = nullptr) {
         const PlanT<R> &pl = plan_x<R>();
         const int pe = prof_begin();
         switch (pl.M) {
-            case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch); break;
-            case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch); break;
-            case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch); break;
-            case 384: xpass_t<MixDst<384, R>>(pl, in, out, nbatch); break;
-            default: xpass_t<GenericDst<R>>(pl, in, out, nbatch); break;
+            case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch, rows); break;
+            case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch, rows); break;
+            case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch, rows); break;
+            case 384: xpass_t<MixDst<384, R>>(pl, in, out, nbatch, rows); break;
+            default: xpass_t<GenericDst<R>>(pl, in, out, nbatch, rows); break;
         }
         check_launch();
         prof_end(pe, IBPM_KCLASS_XPASS, 2.0 * sizeof(R) * (double)ng * nbatch);
@@ -482,9 +483,13 @@ struct Engine final : ibpm_handle {
     // vort2flux (src/fluid.jl:178-205) over nbatch independent fields.
     // G, psi: level 1 of batch 0, level stride ng, batch stride bs.
     // qout: level 1 of batch 0 (level stride nq, batch stride qbs); curl_all=false
-    // computes q only at level 1 (the only level a caller reads).
+    // computes q only at level 1 (the only level a caller reads).  win (device,
+    // with curl_all=false): the level-1 faces the caller reads (E's support, the
+    // body's bbox); level 1's last X pass and curl then skip what lies outside,
+    // leaving those rows of psi and faces of q unwritten.
     void vort2flux(T *psi_, T *qout, T *Gm, long long bs, long long qbs, int nbatch, bool curl_all,
-                   bool hi1 = false) {
+                   bool hi1 = false, const int *win = nullptr) {
+        if (curl_all) win = nullptr;
         for (int lev = 2; lev <= L; ++lev) {
             const int nx2 = nx / 2, ny2 = ny / 2;
             const dim3 blk(16, 16), grd((nx2 + 15) / 16, (ny2 + 15) / 16, nbatch);
@@ -514,13 +519,14 @@ struct Engine final : ibpm_handle {
             else
                 xpass(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, out_plain(t1, ng), nbatch);
             ypass(t1, t2, ng, nbatch, mult(MULT_LAPINV, 1, 0));
-            xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch);
+            xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch, lev == 1 ? win : nullptr);
             if (curl_all || lev == 1) {
                 const dim3 blk(64, 4);
                 const dim3 grd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, nbatch);
                 const int pe = prof_begin();
                 curl_kernel<T, T, T><<<grd, blk, 0, st>>>(qout + (lev - 1) * nq, qbs, Pl, bs,
-                                                          lev < L ? psi_ + lev * ng : nullptr, bs, g);
+                                                          lev < L ? psi_ + lev * ng : nullptr, bs, g,
+                                                          lev == 1 ? win : nullptr);
                 check_launch();
                 prof_end(pe, IBPM_KCLASS_CURL, 8.0 * (double)(ng + nq) * nbatch);
             }
@@ -543,7 +549,7 @@ struct Engine final : ibpm_handle {
         if (L > 1)
             CK(cudaMemset2DAsync(Gw + ng, (size_t)(ng * L) * sizeof(T), 0, (size_t)(ng * (L - 1)) * sizeof(T), nbatch,
                                  st));
-        vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false);
+        vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false, false, P.bbox);  // E reads the bbox only
         launch_regT(P, qw, nq, x, xs, nbatch, 0, prm, g, st);
         check_launch();
     }
@@ -1222,7 +1228,7 @@ void Engine<T>::step_body() {
         vort2flux(psi, qs1, Gnew, 0, 0, 1, false, true);
         launch_regT(P, qs1_hi, 0, Ftmp, 0, 1, 1, prm, g, st);
     } else {
-        vort2flux(psi, qs1, Gnew, 0, 0, 1, false);
+        vort2flux(psi, qs1, Gnew, 0, 0, 1, false, false, P.bbox);  // E reads the bbox only
         launch_regT(P, qs1, 0, Ftmp, 0, 1, 1, prm, g, st);
     }
     check_launch();

@@ -144,9 +144,16 @@ struct Mult {
 
 // X pass: DST along x of rows (ja, jb) = (2p+1, 2p+2) of each batch field.
 // D is the line transform (Pow2Dst<M> or GenericDst); NG line pairs per block.
+// rows (device, may be null): the body's face window i0, i1, j0, j1; a block
+// none of whose rows lies in j0-1 .. j1 (the rows a curl of those faces reads)
+// returns at once and leaves its output rows unwritten.
 template <class D, int NG, class In, class Out>
 __global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
-    xpass_kernel(In in, Out out, PlanT<typename D::Real> pl, int nrows) {
+    xpass_kernel(In in, Out out, PlanT<typename D::Real> pl, int nrows, const int *__restrict__ rows = nullptr) {
+    if (rows != nullptr) {  // uniform over the block: before any barrier
+        const int r0 = 2 * NG * (int)blockIdx.x + 1, r1 = r0 + 2 * NG - 1;
+        if (r1 < rows[2] - 1 || r0 > rows[3]) return;
+    }
     using T = typename D::Real;
     using C = typename D::C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -628,15 +635,17 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a
 // One thread per (i, j) writes both faces there: the x face u(i, j) (i <= nx+1,
 // j <= ny) and the y face v(i, j) (i <= nx, j <= ny+1); inside the ring they share
 // psi(i-1, j-1).  Batch b (blockIdx.z) uses psi + b*bs, q + b*qbs, coarse + b*cbs.
+// win (device, may be null): only the faces in i0..i1 x j0..j1 are written.
 template <class T, class TP, class TC>
 __global__ void curl_kernel(T *__restrict__ qout, long long qbs, const TP *__restrict__ psi, long long bs,
-                            const TC *__restrict__ coarse, long long cbs, Grid g) {
+                            const TC *__restrict__ coarse, long long cbs, Grid g, const int *__restrict__ win = nullptr) {
     const int nx = g.nx, ny = g.ny;
     const long long nu = (long long)(nx + 1) * ny;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int b = blockIdx.z;
     if (i > nx + 1 || j > ny + 1) return;
+    if (win != nullptr && (i < win[0] || i > win[1] || j < win[2] || j > win[3])) return;
     const TP *Pt = psi + b * bs;
     const TC *C = coarse ? coarse + b * cbs : nullptr;
     T *q = qout + b * qbs;
