@@ -347,25 +347,25 @@ struct Engine final : ibpm_handle {
     // Dispatch on the transform length: compile-time transforms for
     // M in {256, 384, 512, 1024}, the runtime mixed-radix one otherwise.
     template <class D, class In, class Out>
-    void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch, const int *rows) {
+    void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch, const int *rows, int zero_outside) {
         const int pairs = (ny - 1 + 1) / 2;
         const dim3 grid((pairs + kNG - 1) / kNG, nbatch);
         const size_t sm = pass_smem<D>(pl.M, kNG, kNG);
-        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, pl, ny - 1, rows);
+        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, pl, ny - 1, rows, zero_outside);
     }
     // X pass with transforms of element type R (the engine's T, or double for
     // the FP32 engine's FP64 level-1 solve); In/Out convert at the boundary.
-    // rows: see xpass_kernel (null: every row).
+    // rows, zero_outside: see xpass_kernel (rows null: every row).
     template <class R = T, class In, class Out>
-    void xpass(In in, Out out, int nbatch, const int *rows = nullptr) {
+    void xpass(In in, Out out, int nbatch, const int *rows = nullptr, int zero_outside = 0) {
         const PlanT<R> &pl = plan_x<R>();
         const int pe = prof_begin();
         switch (pl.M) {
-            case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch, rows); break;
-            case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch, rows); break;
-            case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch, rows); break;
-            case 384: xpass_t<MixDst<384, R>>(pl, in, out, nbatch, rows); break;
-            default: xpass_t<GenericDst<R>>(pl, in, out, nbatch, rows); break;
+            case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch, rows, zero_outside); break;
+            case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch, rows, zero_outside); break;
+            case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch, rows, zero_outside); break;
+            case 384: xpass_t<MixDst<384, R>>(pl, in, out, nbatch, rows, zero_outside); break;
+            default: xpass_t<GenericDst<R>>(pl, in, out, nbatch, rows, zero_outside); break;
         }
         check_launch();
         prof_end(pe, IBPM_KCLASS_XPASS, 2.0 * sizeof(R) * (double)ng * nbatch);
@@ -543,7 +543,7 @@ struct Engine final : ibpm_handle {
     void apply_B(const double *z, double *x, long long xs, int nbatch) {
         reg_patch(z, nbatch);
         InRegRot<T> in{Patch<T>{patch, P.bbox, patch_stride}};
-        xpass(in, out_plain(t1, ng), nbatch);
+        xpass(in, out_plain(t1, ng), nbatch, P.bbox, 1);  // rot of the patch: zero outside its rows
         ypass(t1, t2, ng, nbatch, mult(MULT_AIMPL, 1, 0));
         xpass(in_plain(t2, ng), out_plain(Gw, ng * L), nbatch);
         if (L > 1)
@@ -1292,7 +1292,7 @@ void Engine<T>::step_body() {
     }
     // project_circ (src/coupling.jl:218-230): Gamma = Gamma_s; Gamma_1 -= Ainv_1 rot(E^T F~b)
     reg_patch(Fbt, 1);
-    xpass(InRegRot<T>{Patch<T>{patch, P.bbox, patch_stride}}, out_plain(t1, ng), 1);
+    xpass(InRegRot<T>{Patch<T>{patch, P.bbox, patch_stride}}, out_plain(t1, ng), 1, P.bbox, 1);
     ypass(t1, t2, ng, 1, mult(MULT_AIMPL, 1, 0));
     xpass(in_plain(t2, ng), OutSub<T>{Gnew, ng, nx - 1}, 1);
     // vort2flux!(state.psi, state.q, state.Gamma)

@@ -144,15 +144,25 @@ struct Mult {
 
 // X pass: DST along x of rows (ja, jb) = (2p+1, 2p+2) of each batch field.
 // D is the line transform (Pow2Dst<M> or GenericDst); NG line pairs per block.
-// rows (device, may be null): the body's face window i0, i1, j0, j1; a block
-// none of whose rows lies in j0-1 .. j1 (the rows a curl of those faces reads)
-// returns at once and leaves its output rows unwritten.
+// rows (device, may be null): the body's face window i0, i1, j0, j1.  A block
+// none of whose rows lies in j0-1 .. j1 returns at once: with zero_outside = 0
+// its output rows stay unwritten (the rows a curl of those faces reads lie
+// inside), with zero_outside = 1 it writes them as zeros (the transform of the
+// input's zero rows: rot of a patch inside the window is zero outside them).
 template <class D, int NG, class In, class Out>
 __global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
-    xpass_kernel(In in, Out out, PlanT<typename D::Real> pl, int nrows, const int *__restrict__ rows = nullptr) {
+    xpass_kernel(In in, Out out, PlanT<typename D::Real> pl, int nrows, const int *__restrict__ rows = nullptr,
+                 int zero_outside = 0) {
     if (rows != nullptr) {  // uniform over the block: before any barrier
         const int r0 = 2 * NG * (int)blockIdx.x + 1, r1 = r0 + 2 * NG - 1;
-        if (r1 < rows[2] - 1 || r0 > rows[3]) return;
+        if (r1 < rows[2] - 1 || r0 > rows[3]) {
+            if (zero_outside) {
+                const int t = threadIdx.x % D::TPF, ja = r0 + 2 * (int)(threadIdx.x / D::TPF);
+                for (int jj = ja; jj <= ja + 1 && jj <= nrows; ++jj)
+                    for (int i = 1 + t; i < pl.M; i += D::TPF) out((int)blockIdx.y, i, jj, 0.0);
+            }
+            return;
+        }
     }
     using T = typename D::Real;
     using C = typename D::C;
