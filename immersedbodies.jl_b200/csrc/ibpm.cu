@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -342,6 +343,13 @@ struct Engine final : ibpm_handle {
         ++launches;
         CK(cudaGetLastError());
     }
+    // cudaFuncSetAttribute holds for the current device only: a kernel's launch
+    // site records the devices it set an attribute on (devices >= 64 set it every time)
+    unsigned long long device_bit() const { return device < 64 ? 1ull << device : 0ull; }
+    bool need_attr(const std::atomic<unsigned long long> &done) const {
+        const unsigned long long bit = device_bit();
+        return bit == 0 || !(done.load() & bit);
+    }
 
     // ---- line passes ----
     // Dispatch on the transform length: compile-time transforms for
@@ -390,10 +398,11 @@ struct Engine final : ibpm_handle {
         const dim3 grid((nx - 1 + 2 * NGY - 1) / (2 * NGY), nbatch);
         const size_t sm = pass_smem<D>(pl.M, NGY, NGY);
         if (sm > 48 * 1024) {
-            static bool attr = false;  // one M per compile-time transform, so one size
-            if (!attr) {
+            // one M per compile-time transform, so one size; the attribute is per device
+            static std::atomic<unsigned long long> attr_devices{0};
+            if (need_attr(attr_devices)) {
                 CK(cudaFuncSetAttribute(ypass_kernel<D, NGY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                attr = true;
+                attr_devices.fetch_or(device_bit());
             }
         }
         ypass_kernel<D, NGY><<<grid, NGY * D::TPF, sm, st>>>(in, out, bs, nx - 1, pl, m);
@@ -438,12 +447,13 @@ struct Engine final : ibpm_handle {
         {
             const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), L);
             const size_t sm = pass_smem<D>(ply.M, 2 * kNG, kNG);
-            // the cap must cover the largest M this instantiation serves (kMaxM)
-            static bool attr = false;
-            if (!attr) {
+            // the cap must cover the largest M this instantiation serves (kMaxM); the
+            // attribute is per device
+            static std::atomic<unsigned long long> attr_devices{0};
+            if (need_attr(attr_devices)) {
                 const int cap = (int)pass_smem<D>(kMaxM, 2 * kNG, kNG);
                 CK(cudaFuncSetAttribute(ypass_trial_kernel<D, kNG>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-                attr = true;
+                attr_devices.fetch_or(device_bit());
             }
             const int pe = prof_begin();
             ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1, t2, rhs, ng, nx - 1, ply,
