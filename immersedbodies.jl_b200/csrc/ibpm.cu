@@ -266,36 +266,41 @@ struct Engine final : ibpm_handle {
     // grows the column-batch buffers to kb columns (the projected warm start
     // applies B to all kept solutions in one batched pass)
     void grow_batch_buffers(int kb) {
-        if (kb <= kbatch) return;
-        CK(cudaStreamSynchronize(st));
-        for (void *p : {(void *)t1, (void *)t2, (void *)patch, (void *)Gw, (void *)psiw, (void *)qw, (void *)fcol})
-            dfree(p);
-        kbatch = kb;
-        const int k2 = std::max(kbatch, L);
-        t1 = dalloc<T>(ng * k2);
-        t2 = dalloc<T>(ng * k2);
-        patch = dalloc<T>(patch_stride * kbatch);
-        Gw = dalloc<T>(ng * L * kbatch);
-        psiw = dalloc<T>(ng * L * kbatch);
-        qw = dalloc<T>(nq * kbatch);
-        fcol = dalloc<double>(2 * (size_t)np * kbatch);
+        if (kb > kbatch) resize_batch_buffers(kb);
     }
     // After the B^-1 setup a static-body handle applies B to one vector at a time:
     // the setup's column-batch buffers shrink to one column.
     void shrink_batch_buffers() {
-        if (kbatch <= 1) return;
+        if (kbatch > 1) resize_batch_buffers(1);
+    }
+    // Column-batch work buffers for kb columns.  The new buffers are allocated
+    // before the old ones are freed, so a failed allocation leaves the handle as
+    // it was; the captured graphs, which hold the old addresses, are dropped.
+    void resize_batch_buffers(int kb) {
         CK(cudaStreamSynchronize(st));
+        const int k2 = std::max(kb, L);
+        const size_t sizes[7] = {sizeof(T) * (size_t)(ng * k2),        sizeof(T) * (size_t)(ng * k2),
+                                 sizeof(T) * (size_t)(patch_stride * kb), sizeof(T) * (size_t)(ng * L * kb),
+                                 sizeof(T) * (size_t)(ng * L * kb),     sizeof(T) * (size_t)(nq * kb),
+                                 sizeof(double) * 2 * (size_t)np * kb};
+        void *fresh[7] = {};
+        try {
+            for (int k = 0; k < 7; ++k) fresh[k] = dalloc<unsigned char>(sizes[k]);
+        } catch (...) {
+            for (void *p : fresh) dfree(p);
+            throw;
+        }
+        drop_graphs();
         for (void *p : {(void *)t1, (void *)t2, (void *)patch, (void *)Gw, (void *)psiw, (void *)qw, (void *)fcol})
             dfree(p);
-        kbatch = 1;
-        const int kb = std::max(1, L);
-        t1 = dalloc<T>(ng * kb);
-        t2 = dalloc<T>(ng * kb);
-        patch = dalloc<T>(patch_stride);
-        Gw = dalloc<T>(ng * L);
-        psiw = dalloc<T>(ng * L);
-        qw = dalloc<T>(nq);
-        fcol = dalloc<double>(2 * (size_t)np);
+        t1 = static_cast<T *>(fresh[0]);
+        t2 = static_cast<T *>(fresh[1]);
+        patch = static_cast<T *>(fresh[2]);
+        Gw = static_cast<T *>(fresh[3]);
+        psiw = static_cast<T *>(fresh[4]);
+        qw = static_cast<T *>(fresh[5]);
+        fcol = static_cast<double *>(fresh[6]);
+        kbatch = kb;
     }
 
     template <class U>
@@ -303,7 +308,10 @@ struct Engine final : ibpm_handle {
         void *p = nullptr;
         if (n == 0) n = 1;
         cudaError_t e = cudaMalloc(&p, n * sizeof(U));
-        if (e != cudaSuccess) throw ApiError{IBPM_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(U)) + " bytes failed"};
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();  // not sticky: clear it so later launch checks do not report it
+            throw ApiError{IBPM_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(U)) + " bytes failed"};
+        }
         allocs.push_back(p);
         alloc_bytes.push_back((long long)(n * sizeof(U)));
         dev_bytes += (long long)(n * sizeof(U));
