@@ -260,6 +260,51 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
             "steps_per_s_vs_previous": {m: out[m]["steps_per_s"] / base["steps_per_s"] for m in out}}
 
 
+def mixed_precision_plate_report(ib, device: int, steps: int = 200, timed: int = 50):
+    """The mixed-precision workload as configured: flat plate of chord 1 at 30 deg,
+    Re 200, 1024^2 cells x 5 levels, 201 points, dt 0.001, from rest.  FP64 and
+    FP32 engines are stepped side by side for `steps` steps; the largest
+    |dC_D|, |dC_L| over those steps and over their second half, past the impulsive
+    start (C = 2F / (U^2 c), U = c = 1), and the vorticity relative L2 at the end
+    are reported, then each engine's steps/s over `timed` further steps (CUDA
+    events on its stream)."""
+    import torch
+
+    prob = ib.configs.plate_aoa30_1024()
+    s64 = ib.GpuCnabSolver(ib.State(prob), device=device)
+    s32 = ib.GpuCnabSolver(ib.State(prob), device=device, precision="fp32")
+    dmax, cmax, dlate = 0.0, 0.0, 0.0
+    for k in range(steps):
+        s64.advance_()
+        s32.advance_()
+        c64, c32 = 2 * np.asarray(s64.total_force()), 2 * np.asarray(s32.total_force())
+        d = float(np.abs(c64 - c32).max())
+        dmax = max(dmax, d)
+        cmax = max(cmax, float(np.abs(c64).max()))
+        if 2 * k >= steps:
+            dlate = max(dlate, d)
+    g64, g32 = s64.getstate().Gamma, s32.getstate().Gamma
+    vort = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+
+    def rate(s):
+        stream = torch.cuda.ExternalStream(s.stream_handle())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.advance_many(timed)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return timed / (e0.elapsed_time(e1) / 1000.0)
+
+    v64, v32 = rate(s64), rate(s32)
+    return {"workload": "plate_aoa30_1024: flat plate chord 1 at 30 deg, Re 200, 1024x1024 cells x 5 levels, 201 points, "
+                        "dt 0.001, from rest",
+            "steps_compared": steps, "fp64_steps_per_s": v64, "fp32_steps_per_s": v32, "ratio": v32 / v64,
+            "max_abs_dCD_dCL": dmax, "max_abs_dCD_dCL_second_half": dlate, "max_abs_C": cmax, "vorticity_rel_l2": vort,
+            "bar": "|dC_D|,|dC_L| <= 1e-4 and vorticity rel-L2 <= 1e-5 vs FP64",
+            "meets_bar": bool(dmax <= 1e-4 and vort <= 1e-5)}
+
+
 def direct_start_run(ib, device: int, steps: int, warmup: int):
     """The direct CG start alone (B assembled and inverted on the GPU every step)
     on the 512^2 x 4-level pitching plate at k = 0.55: `warmup` steps, then
@@ -487,6 +532,7 @@ def main():
                   "bar": "|dC_D|,|dC_L| <= 1e-4 and vorticity rel-L2 <= 1e-5 vs FP64",
                   "meets_bar": bool(dC <= 1e-4 and vort <= 1e-5)}
 
+    plate32 = None if args.no_chosen else mixed_precision_plate_report(ib, local)
     learned = None if args.no_learned else warm_start_report(ib, local)
     ensemble = None if args.no_ensemble else ensemble_report(ib, local, seed=2026 + rank)
 
@@ -514,7 +560,8 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps, "api": "GpuCnabSolver.advance_ (ctypes -> ibpm_advance + ibpm_get_forces)"},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-                "chosen_form": chosen, "learned_warm_start": learned, "ensemble": ensemble}
+                "chosen_form": chosen, "chosen_form_plate_aoa30": plate32, "learned_warm_start": learned,
+                "ensemble": ensemble}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
