@@ -305,15 +305,16 @@ def mixed_precision_plate_report(ib, device: int, steps: int = 200, timed: int =
             "meets_bar": bool(dmax <= 1e-4 and vort <= 1e-5)}
 
 
-def direct_start_run(ib, device: int, steps: int, warmup: int):
+def direct_start_run(ib, device: int, steps: int, warmup: int, npts: int = 101):
     """The direct CG start alone (B assembled and inverted on the GPU every step)
-    on the 512^2 x 4-level pitching plate at k = 0.55: `warmup` steps, then
-    `steps` steps timed with CUDA events on the solver's stream, the last of them
-    inside the NVTX range "direct_step" (the range a kernel-launch list selects)."""
+    on the 512^2 x 4-level pitching plate at k = 0.55 with `npts` points (B has
+    2 npts columns): `warmup` steps, then `steps` steps timed with CUDA events on
+    the solver's stream, the last of them inside the NVTX range "direct_step"
+    (the range a kernel-launch list or a profile selects)."""
     import torch
 
-    s = ib.GpuCnabSolver(ib.State(ib.configs.pitching_plate(0.55)), cg=dict(reltol=0.0, abstol=1e-10, maxiter=5000),
-                         device=device)
+    s = ib.GpuCnabSolver(ib.State(ib.configs.pitching_plate(0.55, npts=npts)),
+                         cg=dict(reltol=0.0, abstol=1e-10, maxiter=5000), device=device)
     s.set_warm_start(None, mode="direct", depth=1)
     for _ in range(warmup):
         s.advance_()
@@ -337,7 +338,7 @@ def direct_start_run(ib, device: int, steps: int, warmup: int):
     return {"metric": "moving-body steps/s, direct CG start", "value": 1000.0 / ms, "unit": "steps/s",
             "ms_per_step": ms, "steps": steps, "warmup": warmup, "cg_iterations_mean": float(np.mean(it)),
             "gpu_launches_per_step": (s.kernel_launches() - l0) / steps,
-            "config": {"workload": "pitching_plate_512: 512x512 cells x 4 levels, 101-point plate, Re 500, dt 0.002, "
+            "config": {"workload": f"pitching_plate_512: 512x512 cells x 4 levels, {npts}-point plate, Re 500, dt 0.002, "
                                    "k = 0.55; CG to |r| <= 1e-10", "precision": "fp64"}}
 
 
@@ -408,13 +409,15 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 128-case ensemble measurement")
     ap.add_argument("--direct-start-only", action="store_true",
                     help="time only the moving-body direct CG start (one JSON line) and exit")
+    ap.add_argument("--direct-start-points", type=int, default=101,
+                    help="plate points of --direct-start-only (B has twice as many columns)")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
         return run_reference(args, world, rank)
     if args.direct_start_only:
         ib = load_package()
-        line = direct_start_run(ib, local, args.steps, args.warmup)
+        line = direct_start_run(ib, local, args.steps, args.warmup, args.direct_start_points)
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
