@@ -563,10 +563,10 @@ struct Engine final : ibpm_handle {
         InRegRot<T> in{Patch<T>{patch, P.bbox, patch_stride}};
         xpass(in, out_plain(t1, ng), nbatch, P.bbox, 1);  // rot of the patch: zero outside its rows
         ypass(t1, t2, ng, nbatch, mult(MULT_AIMPL, 1, 0));
+        // Gw's levels 2..L hold the level-1 vorticity coarsified and zeros elsewhere:
+        // vort2flux's coarsify rewrites their central block, and nothing else ever
+        // writes them, so the zeros of the allocation stay
         xpass(in_plain(t2, ng), out_plain(Gw, ng * L), nbatch);
-        if (L > 1)
-            CK(cudaMemset2DAsync(Gw + ng, (size_t)(ng * L) * sizeof(T), 0, (size_t)(ng * (L - 1)) * sizeof(T), nbatch,
-                                 st));
         vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false, false, P.bbox);  // E reads the bbox only
         launch_regT(P, qw, nq, x, xs, nbatch, 0, prm, g, st);
         check_launch();
@@ -615,7 +615,7 @@ struct Engine final : ibpm_handle {
     void init(const ibpm_problem *p, const ibpm_options &o);
     bool hi_level1 = false;
     ibpm_problem problem_copy{};
-    T *diag_q = nullptr;
+    T *diag_q = nullptr, *diag_g = nullptr;  // diag_vort2flux buffers
     void set_state(const ibpm_state_view *s) override;
     void get_field(int field, int level, double *out) override;
     double *field_d = nullptr;  // one level of an output field
@@ -1705,10 +1705,13 @@ template <class T>
 void Engine<T>::diag_vort2flux(double *gamma, double *psi_out, double *q_out) {
     CK(cudaSetDevice(device));
     const size_t ngL = (size_t)(ng * L);
-    upload(Gw, gamma, ngL);
+    // its own vorticity buffer: Gw's coarse levels must stay zero outside the
+    // coarsified block (apply_B relies on it)
+    if (!diag_g) diag_g = dalloc<T>(ngL);
+    upload(diag_g, gamma, ngL);
     if (!diag_q) diag_q = dalloc<T>(nq * L);
-    vort2flux(psiw, diag_q, Gw, 0, 0, 1, true);
-    download(gamma, Gw, ngL);
+    vort2flux(psiw, diag_q, diag_g, 0, 0, 1, true);
+    download(gamma, diag_g, ngL);
     download(psi_out, psiw, ngL);
     download(q_out, diag_q, (size_t)(nq * L));
     CK(cudaStreamSynchronize(st));
