@@ -652,7 +652,7 @@ struct Engine final : ibpm_handle {
     void assemble_invert_B();
     void direct_rebuild();
     int batch_width() const;
-    void cg(double *x, const double *b, bool have_bx = false, bool precond = false);
+    void cg(double *x, const double *b, bool have_bx = false, bool precond = false, const double *rref = nullptr);
     void cg_collect();
     int *cg_it = nullptr;
     bool cg_pending = false, cg_hit_maxiter = false;
@@ -919,6 +919,8 @@ namespace {
 // Device-resident CG state: s[0] = ||r||, s[1] = previous ||r||, s[2] = tol,
 // s[3] = 1 while iterating; it[0] = iterations; err[2] = 1 on a non-finite residual.
 // Preconditioned (pre = 1): s[8] = rho = r . z of the last direction, z = M r in z.
+// rref (device, may be null): the residual norm the relative tolerance scales
+// instead of ||r0|| (the reference start's, when CG starts elsewhere).
 struct CgArgs {
     int n;
     double *x, *r, *u, *c;
@@ -929,6 +931,7 @@ struct CgArgs {
     double reltol, abstol;
     int pre;
     double *z;
+    const double *rref;
 };
 
 __device__ __forceinline__ double cg_block_sum(double v, double *red) {
@@ -955,7 +958,7 @@ __global__ void cg_init_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h
     const double t = cg_block_sum(acc, red);
     if (threadIdx.x == 0) {
         const double res = sqrt(t);
-        const double tol = fmax(a.reltol * res, a.abstol);
+        const double tol = fmax(a.reltol * (a.rref ? *a.rref : res), a.abstol);
         int cont = !(0 >= a.maxiter || res <= tol);
         if (!isfinite(res)) {
             a.err[2] = 1;
@@ -970,6 +973,19 @@ __global__ void cg_init_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h
         a.it[0] = 0;
         if (use_h) cudaGraphSetConditional(h, cont ? 1u : 0u);
     }
+}
+
+// ||b - c|| into *out (one block, the reduction of cg_init_kernel)
+__global__ void residual_norm_kernel(const double *__restrict__ b, const double *__restrict__ c, int n,
+                                     double *__restrict__ out) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const double v = b[k] - c[k];
+        acc += v * v;
+    }
+    const double t = cg_block_sum(acc, red);
+    if (threadIdx.x == 0) *out = sqrt(t);
 }
 
 // u = r + beta u, beta = ||r||^2 / ||r_prev||^2
@@ -1048,11 +1064,11 @@ __global__ void cg_update_kernel(CgArgs a, cudaGraphConditionalHandle h, int use
 // capture the loop is a graph WHILE node whose condition the update kernel
 // sets; otherwise the host reads the condition after every iteration.
 template <class T>
-void Engine<T>::cg(double *x, const double *b, bool have_bx, bool precond) {
+void Engine<T>::cg(double *x, const double *b, bool have_bx, bool precond, const double *rref) {
     const int n = 2 * np;
     const int nchunk = (n + 63) / 64;
     CgArgs a{n, x, cg_r, cg_u, cg_c, b, cg_s, cg_it, err, opt.cg_maxiter, opt.cg_reltol, opt.cg_abstol, precond ? 1 : 0,
-             cg_z};
+             cg_z, rref};
     // the direction: plain, or preconditioned by Binv (z = Binv r)
     auto direction = [&]() {
         if (precond) {
@@ -1271,13 +1287,22 @@ void Engine<T>::step_body() {
         } else if (uses_binv_start()) {
             // x0 = B^-1 b with the inverse of this step's B (or, between rebuilds,
             // of a recent step's); CG then runs from x0, preconditioned by the
-            // same inverse in IBPM_WS_PRECONDITIONED
+            // same inverse in IBPM_WS_PRECONDITIONED.  A relative tolerance keeps
+            // the reference's value, reltol ||b - B F1|| with F1 its start (the
+            // previous solution): x0's own residual is at rounding level.
+            const double *rref = nullptr;
+            if (opt.cg_reltol > 0) {
+                apply_B(Fbt, cg_c, n, 1);
+                residual_norm_kernel<<<1, 256, 0, st>>>(Ftmp, cg_c, n, cg_s + 7);
+                check_launch();
+                rref = cg_s + 7;
+            }
             const int nchunk = (n + 63) / 64;
             binv_gemv_kernel<<<dim3(nchunk, nchunk), 256, 0, st>>>(Binv, Ftmp, part, n);
             check_launch();
             binv_reduce_kernel<<<1, 1024, 0, st>>>(part, nchunk, n, Fbt, fb, total, g.h, g.dt, 1);
             check_launch();
-            cg(Fbt, Ftmp, false, ws_mode == IBPM_WS_PRECONDITIONED);
+            cg(Fbt, Ftmp, false, ws_mode == IBPM_WS_PRECONDITIONED, rref);
         } else if (ws_mode == IBPM_WS_PROJECTED) {
             // Galerkin over the last ws_depth solutions, B applied to all in one batch
             apply_B(ws_hist, ws_bhist, 2 * np, ws_depth);

@@ -41,6 +41,29 @@ def test_gpu_matches_golden(ib, path):
         assert abs(s.info().last_cg_iters - int(fx["cg_iters"])) <= 1
 
 
+@pytest.mark.parametrize("mode,depth", [("direct", 1), ("preconditioned", 2)])
+def test_gpu_fast_force_solves_match_golden_moving_plate(ib, mode, depth):
+    """The direct start and the preconditioned CG on the moving-plate fixture with
+    the reference's CG options (reltol 1e-12, abstol 0).  The relative tolerance
+    keeps the reference's value, 1e-12 of its own start's residual, so CG stops
+    after a few iterations instead of chasing the rounding-level residual of
+    B^-1 b; the iterates differ from the reference's, so state and forces agree
+    to the CG tolerance times B's conditioning, not to the drop-in bar."""
+    fx = np.load(os.path.join(GOLD, "plate32_moving.npz"))
+    prob, st = problem_from_fixture(ib, fx)
+    s = ib.create_solver(st)
+    s.set_warm_start(None, mode=mode, depth=depth)
+    forces, iters = [], []
+    for _ in range(int(fx["nsteps"])):
+        s.advance_()
+        forces.append(st.fb.sum(axis=0).copy())
+        iters.append(s.info().last_cg_iters)
+    s.getstate()
+    assert max(iters) <= 20, iters  # the reference's start takes 75
+    assert rel_l2(st.Gamma, fx["Gamma"]) <= 1e-8
+    assert np.abs(np.array(forces) - fx["forces"]).max() <= 1e-7 * np.abs(fx["forces"]).max()
+
+
 def test_gpu_matches_oracle_cylinder_200(ib, orc):
     """The 200x200, 3-level, 157-point cylinder at Re 100, dt 0.004 (the reference's CPU case), 30 steps."""
     nsteps = 30
