@@ -1306,13 +1306,27 @@ void Engine<T>::step_body() {
         } else if (ws_mode == IBPM_WS_PROJECTED) {
             // Galerkin over the last ws_depth solutions, B applied to all in one batch
             apply_B(ws_hist, ws_bhist, 2 * np, ws_depth);
+            // slot 0 holds F1, the reference's start: its residual scales reltol
+            const double *rref = nullptr;
+            if (opt.cg_reltol > 0) {
+                residual_norm_kernel<<<1, 256, 0, st>>>(Ftmp, ws_bhist, n, cg_s + 7);
+                check_launch();
+                rref = cg_s + 7;
+            }
             launch_ws_projection(ws_hist, ws_bhist, Ftmp, Fbt, cg_c, 2 * np, ws_depth, ws_G, ws_h, cg_s + 5, st);
             check_launch();
-            cg(Fbt, Ftmp, true);
+            cg(Fbt, Ftmp, true, false, rref);
             launch_ws_shift(ws_hist, Fbt, 2 * np, ws_depth, st);
             check_launch();
         } else {
             apply_B(ws_z, ws_bz, 2 * np, 2);
+            // ws_z's first column is F1, the reference's start: its residual scales reltol
+            const double *rref = nullptr;
+            if (opt.cg_reltol > 0) {
+                residual_norm_kernel<<<1, 256, 0, st>>>(Ftmp, ws_bz, n, cg_s + 7);
+                check_launch();
+                rref = cg_s + 7;
+            }
             launch_ws_galerkin(ws_z, ws_bz, Ftmp, Fbt, cg_c, ws_x2, ws_bx2, np, 1, cg_s + 5, st);
             check_launch();
             launch_ws_features(Ftmp, cg_c, ws_z, ws_z + 2 * np, P.ub, motion, pbody_d, np, ws_feat, ws_x2 + 4 * np,
@@ -1327,7 +1341,7 @@ void Engine<T>::step_body() {
                 launch_ws_galerkin(ws_x2, ws_bx2, Ftmp, Fbt, cg_c, nullptr, nullptr, np, 1, cg_s + 6, st);
                 check_launch();
             }
-            cg(Fbt, Ftmp, true);
+            cg(Fbt, Ftmp, true, false, rref);
         }
         cg_pending = true;
         binv_reduce_kernel<<<1, 1024, 0, st>>>(nullptr, 0, n, Fbt, fb, total, g.h, g.dt, 0);

@@ -267,15 +267,14 @@ const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed
  *                         inverse (z = B_k^-1 r, B_k of the last rebuild): between
  *                         rebuilds CG needs a few iterations instead of hundreds.
  *                         Not the reference's iteration (it passes no
- *                         preconditioner); the stopping rule on ||r|| is the same.
- *                         In both modes a relative tolerance keeps the reference's
- *                         value, reltol ||b - B F1|| (F1 the previous solution, one
- *                         more application of B per step), since the guess's own
- *                         residual is at rounding level
+ *                         preconditioner); the stopping rule on ||r|| is the same
  * where the coefficients minimise the B-energy norm of the error over their
  * directions (Galerkin steps with B of the current step, applied in batched
- * passes; CG reuses B x0).  CG then runs from the guess to its tolerance in
- * every mode. */
+ * passes; CG reuses B x0).  CG then runs from the guess to the reference's
+ * tolerance in every mode: max(reltol ||b - B F1||, abstol), the relative part
+ * taken from the residual at the reference's own start F1 (the direct and
+ * preconditioned modes apply B to F1 once more for it when reltol > 0), so a
+ * better guess changes only the iteration count. */
 #define IBPM_WS_PREVIOUS 0
 #define IBPM_WS_LEARNED 1
 #define IBPM_WS_EXTRAPOLATED 2

@@ -172,6 +172,28 @@ def test_direct_start_inverts_the_current_B(ib):
     assert np.abs(Binv @ B - np.eye(n)).max() <= 1e-8
 
 
+def test_every_start_keeps_the_reference_relative_tolerance(ib):
+    """With the reference's CG options (reltol 1e-12 of the residual at its start
+    F1, abstol 0) every start stops at the tolerance the reference's start sets,
+    so a better start needs fewer iterations, never more, and all reach the same
+    forces."""
+    cg = dict(reltol=1e-12, abstol=0.0, maxiter=5000)
+    res = {}
+    for mode, depth in (("previous", 8), ("extrapolated", 8), ("projected", 8), ("direct", 1), ("preconditioned", 8)):
+        prob = ib.configs.pitching_plate(0.5, h=0.04, n=128, nlevel=3, npts=26, dt=0.004)
+        s = ib.GpuCnabSolver(ib.State(prob), cg=cg)
+        if mode != "previous":
+            s.set_warm_start(None, mode=mode, depth=depth)
+        it = _iters(s, 30)
+        res[mode] = (it[10:].mean(), s.total_force().copy())
+        del s
+    it0, f0 = res["previous"]
+    for mode, (it, f) in res.items():
+        assert it <= 1.02 * it0 + 1, (mode, it, it0)
+        assert np.abs(f - f0).max() <= 1e-7 * np.abs(f0).max(), mode
+    assert res["direct"][0] <= 2 and res["preconditioned"][0] <= 10
+
+
 def test_learned_warm_start_on_a_held_out_frequency(ib, capsys):
     """Trained on samples of k = 0.3 and 0.7, run at k = 0.5.  The learned start
     includes the extrapolation step, so it must use fewer CG iterations than the
