@@ -17,7 +17,6 @@ import argparse
 import importlib.util
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -57,19 +56,15 @@ def step_bytes_model(nx: int, ny: int, L: int, npanel: int, s: float = 1.0) -> f
             + 8.0 * (2 * npanel) ** 2)
 
 
-def read_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from its committed ncu summary (a line
-    `traffic_bytes_per_launch: N`), or None when no summary exists."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_cylinder_re100_1024.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                m = re.match(r"\s*traffic_bytes_per_launch:\s*([0-9.eE+]+)", line)
-                if m:
-                    return float(m.group(1)), os.path.relpath(path, ROOT)
-    except OSError:
-        pass
-    return None, None
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dominant kernel, from one ncu capture (not measured by this run):
+#   ncu --set full --clock-control none -k regex:ypass_kernel -s 210 -c 1 \
+#       python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-chosen --no-learned --no-ensemble
+# on one B200; cold-cache replay of one single-level Y pass of the 1024^2 x 5 step.
+NCU_TRAFFIC = {"ypass_kernel": 8454912.0}
+NCU_TRAFFIC_RUN = ("ncu --set full capture of one ypass_kernel launch (1023^2 FP64 level) of "
+                   "`python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-chosen --no-learned --no-ensemble`; "
+                   "a constant, not measured by this run")
 
 
 def read_peaks():
@@ -493,11 +488,11 @@ def main():
     n_y, ms_y, b_y = kern["ypass"]
     dom = "ypass_kernel (one level: DST along y, multiply by scale/Λ, DST along y)"
     achieved = (b_y / n_y) / ((ms_y / n_y) / 1000.0) / 1e9 if n_y else None
-    traffic, traffic_src = read_traffic("ypass_kernel")
+    traffic = NCU_TRAFFIC.get("ypass_kernel")
     step_bytes = step_bytes_model(nx, ny, L, prob.bodies.npanel)
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": traffic,
-                "traffic_source": traffic_src and f"dram__bytes_read.sum + dram__bytes_write.sum, ncu ({traffic_src})",
+                "traffic_source": traffic and NCU_TRAFFIC_RUN,
                 "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": b_y / n_y if n_y else None,
                 "launch_ms": ms_y / n_y if n_y else None,

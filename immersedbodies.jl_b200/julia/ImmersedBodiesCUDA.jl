@@ -5,8 +5,9 @@ A drop-in `AbstractSolver` for ImmersedBodies.jl whose `advance!` runs on a B200
 through `libibpm_b200.so` (C ABI: `include/ibpm_b200.h`).
 
     using ImmersedBodies, ImmersedBodiesCUDA
-    solver = GpuCnabSolver(State(prob))      # instead of create_solver(state)
-    solve!(solver; t=1.0)                    # ImmersedBodies' own driver loop
+    solve(prob; t=1.0, solver_kw=(; gpu=true))   # the reference's solve, GPU solver
+    solver = GpuCnabSolver(State(prob))          # or build it by hand
+    solve!(solver; t=1.0)                        # ImmersedBodies' own driver loop
 
 Host callbacks (`freestream_vel(t)`, each `MovingRigidBody`'s `motion(t)`, a
 `MovingGrid`'s `motion(t)`) are evaluated here each step and passed to the
@@ -71,7 +72,7 @@ mutable struct GpuCnabSolver <: AbstractSolver
     stale::Bool
 end
 
-function GpuCnabSolver(state::State{CNAB}; cg=(), device=0)
+function GpuCnabSolver(state::State{CNAB}; cg=(), device=0, fftw=())  # fftw: the CPU solver's option, unused
     prob = state.prob
     bodies = prob.bodies
     parts = bodies.preset
@@ -107,6 +108,21 @@ function GpuCnabSolver(state::State{CNAB}; cg=(), device=0)
 end
 
 create_solver(state::State{CNAB}, ::Val{:gpu}; kw...) = GpuCnabSolver(state; kw...)
+
+# solve(prob; solver_kw) builds its solver with create_solver(State(prob); solver_kw...)
+# (src/solver.jl:71-74, 152), and Julia does not dispatch on keywords.  At load time
+# the reference's create_solver(::State{CNAB}; kw...) is therefore replaced by one
+# that takes a `gpu` keyword: gpu=true builds a GpuCnabSolver (keywords cg, device),
+# gpu=false (the default) builds the reference's CnabSolver exactly as before.  The
+# replacement runs in __init__, not at precompile time, where overwriting another
+# module's method is not allowed.
+function __init__()
+    Core.eval(ImmersedBodies, quote
+        create_solver(state::State{CNAB}; gpu::Bool=false, kw...) =
+            gpu ? $(GpuCnabSolver)(state; kw...) : CnabSolver(state; kw...)
+    end)
+    nothing
+end
 
 function _view(s::State)
     IbpmStateView(s.index, s.t0, pointer(s.q), pointer(s.q0), pointer(s.Γ), pointer(s.ψ),

@@ -26,67 +26,120 @@
 typedef double complex cplx;
 
 /* ------------------------------------------------------------------------- */
-/* FFT (mixed radix, recursive decimation in time)                            */
+/* FFT (mixed radix, iterative Stockham autosort, precomputed twiddles)       */
 /* ------------------------------------------------------------------------- */
+/* Forward transform X_k = sum_j x_j exp(-2 pi i j k / n).  n is factored into
+ * stages of radix 4, 2, 3 and then any other prime; stage s (radix p, Ns the
+ * product of the earlier radices) maps x to y by
+ *   y[q Ns p + k + r Ns] = sum_t W_p^{r t} W_{Ns p}^{t k} x[q Ns + k + t n/p]
+ * for q < n/(Ns p), k < Ns.  Every twiddle W_{Ns p}^{t k} and every root
+ * W_p^{r t} is tabulated when the plan is made (long double), so the transform
+ * does no index modulo and evaluates no trigonometric function. */
+
+#define FFT_MAX_STAGES 40
 
 typedef struct fft_plan {
     int n;
-    cplx *tw; /* tw[k] = exp(-2 pi i k / n) */
+    int nst;
+    int radix[FFT_MAX_STAGES];
+    cplx *tw[FFT_MAX_STAGES];   /* tw[s][k (p-1) + t - 1] = W_{Ns p}^{t k}, k < Ns, 1 <= t < p */
+    cplx *root[FFT_MAX_STAGES]; /* root[s][r p + t] = W_p^{r t} */
 } fft_plan;
 
+static cplx cexpm(long double num, long double den) { /* exp(-2 pi i num / den) */
+    const long double a = -2.0L * 3.14159265358979323846264338327950288L * num / den;
+    return (double)cosl(a) + I * (double)sinl(a);
+}
+
 static fft_plan *fft_plan_new(int n) {
-    fft_plan *p = (fft_plan *)malloc(sizeof(fft_plan));
-    p->n = n;
-    p->tw = (cplx *)malloc(sizeof(cplx) * (size_t)n);
-    for (int k = 0; k < n; k++) {
-        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
-        p->tw[k] = (double)cosl(a) + I * (double)sinl(a);
+    fft_plan *pl = (fft_plan *)calloc(1, sizeof(fft_plan));
+    pl->n = n;
+    int m = n, Ns = 1;
+    while (m > 1) {
+        int p;
+        if (m % 4 == 0)
+            p = 4;
+        else if (m % 2 == 0)
+            p = 2;
+        else {
+            p = m;
+            for (int f = 3; f * f <= m; f += 2)
+                if (m % f == 0) {
+                    p = f;
+                    break;
+                }
+        }
+        const int s = pl->nst++;
+        pl->radix[s] = p;
+        pl->tw[s] = (cplx *)malloc(sizeof(cplx) * (size_t)Ns * (size_t)(p - 1));
+        for (int k = 0; k < Ns; k++)
+            for (int t = 1; t < p; t++) pl->tw[s][(size_t)k * (p - 1) + t - 1] = cexpm((long double)t * k, (long double)Ns * p);
+        pl->root[s] = (cplx *)malloc(sizeof(cplx) * (size_t)p * p);
+        for (int r = 0; r < p; r++)
+            for (int t = 0; t < p; t++) pl->root[s][(size_t)r * p + t] = cexpm((long double)((r * t) % p), (long double)p);
+        Ns *= p;
+        m /= p;
     }
-    return p;
+    return pl;
 }
 
 static void fft_plan_free(fft_plan *p) {
     if (!p) return;
-    free(p->tw);
+    for (int s = 0; s < p->nst; s++) {
+        free(p->tw[s]);
+        free(p->root[s]);
+    }
     free(p);
 }
 
-static int smallest_factor(int n) {
-    if (n % 4 == 0) return 4;
-    for (int f = 2; f * f <= n; f++)
-        if (n % f == 0) return f;
-    return n;
-}
-
-/* out[k] = sum_j in[j*is] W_n^{jk}; tw holds the N-point table, twstep = N/n. */
-static void fft_rec(const cplx *in, int is, cplx *out, int n, const fft_plan *pl, int twstep) {
-    if (n == 1) {
-        out[0] = in[0];
-        return;
-    }
-    int p = smallest_factor(n);
-    int m = n / p;
-    for (int r = 0; r < p; r++) fft_rec(in + (size_t)r * is, is * p, out + (size_t)r * m, m, pl, twstep * p);
-    cplx a[64];
-    cplx *buf = p <= 64 ? a : (cplx *)malloc(sizeof(cplx) * (size_t)p);
-    const int N = pl->n;
-    /* For each k the p inputs out[r m + k] are read into buf before the p
-     * outputs out[k + s m] (the same index set) are written. */
-    for (int k = 0; k < m; k++) {
-        for (int r = 0; r < p; r++) {
-            long e = ((long)r * k * twstep) % N;
-            buf[r] = out[(size_t)r * m + k] * pl->tw[e];
-        }
-        for (int s = 0; s < p; s++) {
-            cplx acc = 0;
-            for (int r = 0; r < p; r++) {
-                long e = ((long)r * s * m * twstep) % N;
-                acc += buf[r] * pl->tw[e];
+/* Forward FFT of x (length pl->n); w is scratch of the same length.  The result
+ * is in x on return. */
+static void fft_exec(const fft_plan *pl, cplx *x, cplx *w) {
+    const int n = pl->n;
+    cplx *src = x, *dst = w;
+    int Ns = 1;
+    for (int s = 0; s < pl->nst; s++) {
+        const int p = pl->radix[s], stride = n / p, nq = n / (Ns * p);
+        const cplx *tw = pl->tw[s], *rt = pl->root[s];
+        for (int q = 0; q < nq; q++) {
+            for (int k = 0; k < Ns; k++) {
+                const int j = q * Ns + k;
+                const cplx *twk = tw + (size_t)k * (p - 1);
+                cplx *out = dst + (size_t)q * Ns * p + k;
+                if (p == 4) {
+                    const cplx a = src[j], b = src[j + stride] * (k ? twk[0] : 1.0);
+                    const cplx c = src[j + 2 * stride] * (k ? twk[1] : 1.0);
+                    const cplx d = src[j + 3 * stride] * (k ? twk[2] : 1.0);
+                    const cplx t0 = a + c, t1 = a - c, t2 = b + d, t3 = -I * (b - d);
+                    out[0] = t0 + t2;
+                    out[Ns] = t1 + t3;
+                    out[2 * Ns] = t0 - t2;
+                    out[3 * Ns] = t1 - t3;
+                } else if (p == 2) {
+                    const cplx a = src[j], b = src[j + stride] * (k ? twk[0] : 1.0);
+                    out[0] = a + b;
+                    out[Ns] = a - b;
+                } else {
+                    cplx v[64];
+                    cplx *vb = p <= 64 ? v : (cplx *)malloc(sizeof(cplx) * (size_t)p);
+                    vb[0] = src[j];
+                    for (int t = 1; t < p; t++) vb[t] = src[j + t * stride] * twk[t - 1];
+                    for (int r = 0; r < p; r++) {
+                        cplx acc = 0;
+                        const cplx *rr = rt + (size_t)r * p;
+                        for (int t = 0; t < p; t++) acc += vb[t] * rr[t];
+                        out[(size_t)r * Ns] = acc;
+                    }
+                    if (vb != v) free(vb);
+                }
             }
-            out[(size_t)k + (size_t)s * m] = acc;
         }
+        cplx *tmp = src;
+        src = dst;
+        dst = tmp;
+        Ns *= p;
     }
-    if (buf != a) free(buf);
+    if (src != x) memcpy(x, src, sizeof(cplx) * (size_t)n);
 }
 
 /* Pairwise DST-I of two real lines a, b of length n (FFTW RODFT00 definition):
@@ -102,10 +155,10 @@ static void dst1_pair(int n, const double *a, int as, const double *b, int bs, d
         z[j] = av + I * bv;
         z[N - j] = -(av + I * bv);
     }
-    fft_rec(z, 1, Z, N, pl, 1);
+    fft_exec(pl, z, Z);
     for (int k = 1; k <= n; k++) {
-        ya[(size_t)(k - 1) * yas] = -cimag(Z[k]);
-        if (yb) yb[(size_t)(k - 1) * ybs] = creal(Z[k]);
+        ya[(size_t)(k - 1) * yas] = -cimag(z[k]);
+        if (yb) yb[(size_t)(k - 1) * ybs] = creal(z[k]);
     }
 }
 
@@ -210,6 +263,7 @@ static double gridstep(const orc_solver *s, int lev) { return ldexp(1.0, lev - 1
 /* rot! (src/fluid.jl:101-111) */
 static void rot(const orc_solver *s, double *G, const double *q) {
     const int nx = s->nx, ny = s->ny;
+#pragma omp parallel for schedule(static)
     for (int j = 2; j <= ny; j++)
         for (int i = 2; i <= nx; i++) GAM(G, i - 1, j - 1) = (QX(q, i, j - 1) - QX(q, i, j)) + (QY(q, i, j) - QY(q, i - 1, j));
 }
@@ -217,6 +271,7 @@ static void rot(const orc_solver *s, double *G, const double *q) {
 /* 4-argument curl! (src/fluid.jl:230-276) */
 static void curl(const orc_solver *s, double *q, const double *psi, const double *pbc) {
     const int nx = s->nx, ny = s->ny, T = s->bT, B = s->bB, L = s->bL, R = s->bR;
+#pragma omp parallel for schedule(static)
     for (int j = 2; j <= ny - 1; j++)
         for (int i = 2; i <= nx; i++) QX(q, i, j) = GAM(psi, i - 1, j) - GAM(psi, i - 1, j - 1);
     for (int i = 2; i <= nx; i++) QX(q, i, 1) = GAM(psi, i - 1, 1) - BC(pbc, B + i);
@@ -224,6 +279,7 @@ static void curl(const orc_solver *s, double *q, const double *psi, const double
     for (int j = 1; j <= ny; j++) QX(q, 1, j) = BC(pbc, (L + 1) + j) - BC(pbc, L + j);
     for (int j = 1; j <= ny; j++) QX(q, nx + 1, j) = BC(pbc, (R + 1) + j) - BC(pbc, R + j);
 
+#pragma omp parallel for schedule(static)
     for (int j = 2; j <= ny; j++)
         for (int i = 2; i <= nx - 1; i++) QY(q, i, j) = GAM(psi, i - 1, j - 1) - GAM(psi, i, j - 1);
     for (int j = 2; j <= ny; j++) QY(q, 1, j) = BC(pbc, L + j) - GAM(psi, 1, j - 1);
@@ -301,6 +357,7 @@ static void lap_inv(const orc_solver *s, const double *Lam, double *x, const dou
     const double scale = 1.0 / (double)(4 * (long)s->nx * (long)s->ny);
     memcpy(s->Gdst1, b, ng * sizeof(double));
     dst2_plans(s->nx - 1, s->ny - 1, s->Gdst1, s->Gdst2, s->plx, s->ply);
+#pragma omp parallel for schedule(static)
     for (size_t k = 0; k < ng; k++) s->Gdst2[k] *= scale / Lam[k];
     dst2_plans(s->nx - 1, s->ny - 1, s->Gdst2, s->Gdst1, s->plx, s->ply);
     memcpy(x, s->Gdst1, ng * sizeof(double));
@@ -340,9 +397,11 @@ static void avg_flux(const orc_solver *s, double *Q, int lev) {
     const size_t nq = (size_t)s->nq;
     const double *q = s->q + nq * (lev - 1), *q0 = s->q0 + nq * (lev - 1);
     memset(Q, 0, sizeof(double) * nq);
+#pragma omp parallel for schedule(static)
     for (int j = 2; j <= ny; j++)
         for (int i = 1; i <= nx + 1; i++)
             QX(Q, i, j) = (QX(q, i, j) + QX(q, i, j - 1) + QX(q0, i, j) + QX(q0, i, j - 1)) / 2;
+#pragma omp parallel for schedule(static)
     for (int j = 1; j <= ny + 1; j++)
         for (int i = 2; i <= nx; i++)
             QY(Q, i, j) = (QY(q, i, j) + QY(q, i - 1, j) + QY(q0, i, j) + QY(q0, i - 1, j)) / 2;
@@ -352,12 +411,14 @@ static void avg_flux(const orc_solver *s, double *Q, int lev) {
 static void direct_product(const orc_solver *s, double *fq, const double *Q, const double *G, const double *Gbc) {
     const int nx = s->nx, ny = s->ny, T = s->bT, B = s->bB, L = s->bL, R = s->bR;
     memset(fq, 0, sizeof(double) * (size_t)s->nq);
+#pragma omp parallel for schedule(static)
     for (int j = 2; j <= ny - 1; j++)
         for (int i = 2; i <= nx; i++)
             QX(fq, i, j) = (QY(Q, i, j + 1) * GAM(G, i - 1, j) + QY(Q, i, j) * GAM(G, i - 1, j - 1)) / 2;
     for (int i = 2; i <= nx; i++) QX(fq, i, 1) = (QY(Q, i, 2) * GAM(G, i - 1, 1) + QY(Q, i, 1) * BC(Gbc, B + i)) / 2;
     for (int i = 2; i <= nx; i++)
         QX(fq, i, ny) = (QY(Q, i, ny) * GAM(G, i - 1, ny - 1) + QY(Q, i, ny + 1) * BC(Gbc, T + i)) / 2;
+#pragma omp parallel for schedule(static)
     for (int j = 2; j <= ny; j++)
         for (int i = 2; i <= nx - 1; i++)
             QY(fq, i, j) = -(QX(Q, i + 1, j) * GAM(G, i, j - 1) + QX(Q, i, j) * GAM(G, i - 1, j - 1)) / 2;
@@ -374,6 +435,7 @@ static void nonlinear(orc_solver *s, double *nl, const double *Gbc, int lev) {
     rot(s, nl, s->qtmp2);
     const double hc = gridstep(s, lev);
     const double f = 1 / (hc * hc);
+#pragma omp parallel for schedule(static)
     for (size_t k = 0; k < ng; k++) nl[k] *= f;
 }
 

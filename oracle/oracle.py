@@ -148,7 +148,7 @@ class OracleSolver:
         ds = np.concatenate([b.panels.ds for _, b, _ in bodies.preset])
         self._keep = (kinds, starts, xb, ds)
         g = prob.grid
-        cg = dict(maxiter=5000, reltol=1e-12, abstol=0.0, **(cg or {}))
+        cg = {"maxiter": 5000, "reltol": 1e-12, "abstol": 0.0, **(cg or {})}
         p = orc_problem(nx=g.base.n[0], ny=g.base.n[1], nlevel=g.nlevel, h=g.base.h, x0=g.base.x0[0],
                         y0=g.base.x0[1], Re=prob.fluid.Re, dt=prob.scheme.dt, npanel=bodies.npanel,
                         nbody=len(kinds), body_kind=kinds.ctypes.data_as(_ip), body_start=starts.ctypes.data_as(_ip),
