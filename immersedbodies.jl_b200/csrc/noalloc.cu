@@ -16,7 +16,14 @@
 //    nx, ny even, <= 1024, of the form 2^a 3^b 5^c; larger sizes are rejected.
 //  * The first call on a device (and any call whose nx/ny differ from that
 //    device's previous call) writes the transform tables into g_scratch; make
-//    that first call before any stream capture.
+//    that first call before any stream capture.  Such a call made while the
+//    stream is capturing is rejected (IBPM_ERR_INVALID): its table kernels would
+//    only enter the graph, and later eager calls would read unwritten tables.
+//  * b and x may be the same buffer: the first pass reads b into scratch and
+//    only the last pass writes x, in stream order.
+//  * Errors are read from each launch's own return code (cudaLaunchKernel), so
+//    an error left pending by an unrelated earlier launch is not reported as
+//    this call's failure.
 //  * Every call shares g_scratch, which keeps the last call's contents: calls
 //    that overlap on the GPU (different streams, or other host threads) race.
 #include <cuda_runtime.h>
@@ -87,17 +94,29 @@ bool plan_ok(int M, PlanT<double> &pl) {
 }
 
 template <class D, class In, class Out>
-void xpass_na(const PlanT<double> &pl, In in, Out out, int nrows, cudaStream_t st) {
+cudaError_t xpass_na(const PlanT<double> &pl, In in, Out out, int nrows, cudaStream_t st) {
     constexpr int NG = 2;
     const dim3 grid(((nrows + 1) / 2 + NG - 1) / NG, 1);
-    xpass_kernel<D, NG, In, Out><<<grid, NG * D::TPF, pass_smem<D>(pl.M, NG, NG), st>>>(in, out, pl, nrows);
+    const int *rows = nullptr;
+    int zero_outside = 0;
+    void *args[] = {&in, &out, const_cast<PlanT<double> *>(&pl), &nrows, &rows, &zero_outside};
+    return cudaLaunchKernel((const void *)xpass_kernel<D, NG, In, Out>, grid, dim3(NG * D::TPF), args,
+                            pass_smem<D>(pl.M, NG, NG), st);
 }
 
 template <class D>
-void ypass_na(const PlanT<double> &pl, const double *in, double *out, int ncols, Mult m, cudaStream_t st) {
+cudaError_t ypass_na(const PlanT<double> &pl, const double *in, double *out, int ncols, Mult m, cudaStream_t st) {
     constexpr int NG = 2;
     const dim3 grid((ncols + 2 * NG - 1) / (2 * NG), 1);
-    ypass_kernel<D, NG><<<grid, NG * D::TPF, pass_smem<D>(pl.M, NG, NG), st>>>(in, out, 0, ncols, pl, m);
+    long long bs = 0;
+    void *args[] = {&in, &out, &bs, &ncols, const_cast<PlanT<double> *>(&pl), &m};
+    return cudaLaunchKernel((const void *)ypass_kernel<D, NG>, grid, dim3(NG * D::TPF), args,
+                            pass_smem<D>(pl.M, NG, NG), st);
+}
+
+cudaError_t tables_na(double2 *tw, double *sn, double *cs, int M, cudaStream_t st) {
+    void *args[] = {&tw, &sn, &cs, &M};
+    return cudaLaunchKernel((const void *)noalloc_tables_kernel, dim3(8), dim3(128), args, 0, st);
 }
 
 }  // namespace
@@ -131,9 +150,15 @@ int ibpm_lap_inv_noalloc(int nx, int ny, const double *b, double *x, void *strea
         double *snx = tab + 4 * kNoAllocMaxM, *sny = snx + (kNoAllocMaxM + 1);
         double *csx = sny + (kNoAllocMaxM + 1), *csy = csx + (kNoAllocMaxM + 1);
         if (slot.nx != nx || slot.ny != ny) {
-            noalloc_tables_kernel<<<8, 128, 0, st>>>(twx, snx, csx, nx);
-            noalloc_tables_kernel<<<8, 128, 0, st>>>(twy, sny, csy, ny);
-            const cudaError_t e = cudaGetLastError();
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            cudaError_t e = cudaStreamIsCapturing(st, &cs);
+            if (e != cudaSuccess) return fail(IBPM_ERR_CUDA, cudaGetErrorString(e));
+            if (cs != cudaStreamCaptureStatusNone)
+                return fail(IBPM_ERR_INVALID,
+                            "the transform tables for this size are not written yet: make the first call for these "
+                            "nx, ny on this device outside stream capture");
+            e = tables_na(twx, snx, csx, nx, st);
+            if (e == cudaSuccess) e = tables_na(twy, sny, csy, ny, st);
             if (e != cudaSuccess) return fail(IBPM_ERR_CUDA, cudaGetErrorString(e));
             slot.nx = nx;
             slot.ny = ny;
@@ -156,10 +181,10 @@ int ibpm_lap_inv_noalloc(int nx, int ny, const double *b, double *x, void *strea
     m.lev0 = 1;
     m.levstep = 0;
     using D = GenericDst<double>;
-    xpass_na<D>(plx, InPlain<double>{b, 0, nx - 1}, OutPlain<double>{t1, 0, nx - 1}, ny - 1, st);
-    ypass_na<D>(ply, t1, t2, nx - 1, m, st);
-    xpass_na<D>(plx, InPlain<double>{t2, 0, nx - 1}, OutPlain<double>{x, 0, nx - 1}, ny - 1, st);
-    const cudaError_t e = cudaGetLastError();
+    cudaError_t e = xpass_na<D>(plx, InPlain<double>{b, 0, nx - 1}, OutPlain<double>{t1, 0, nx - 1}, ny - 1, st);
+    if (e == cudaSuccess) e = ypass_na<D>(ply, t1, t2, nx - 1, m, st);
+    if (e == cudaSuccess)
+        e = xpass_na<D>(plx, InPlain<double>{t2, 0, nx - 1}, OutPlain<double>{x, 0, nx - 1}, ny - 1, st);
     if (e != cudaSuccess) return fail(IBPM_ERR_CUDA, cudaGetErrorString(e));
     return IBPM_OK;
 }

@@ -292,12 +292,14 @@ int ibpm_warm_start_sample(ibpm_handle *h, float *features, float *target, float
  * that cannot allocate device memory.  No counterpart in the reference: it exists
  * for code running inside another framework's memory pool or a fixed arena, or a
  * host loop that must not allocate between steps.  b and x are caller-owned
- * device buffers of (nx-1) x (ny-1) doubles, column-major; x may not alias b.
+ * device buffers of (nx-1) x (ny-1) doubles, column-major; x may be b (the
+ * first pass reads b into scratch, the last writes x, in stream order).
  * The scratch fields and transform tables live in one static device array of
  * about 4.3 MB that each GPU loading the library keeps until exit; it limits
  * (nx-1)(ny-1) to 262144 cells (nx, ny even, <= 1024, of the form 2^a 3^b 5^c).
- * Larger sizes return IBPM_ERR_INVALID.  The first call on a device writes the
- * tables (make it before any stream capture); all calls share the array, so
+ * Larger sizes return IBPM_ERR_INVALID.  The first call on a device (and the
+ * first after a change of nx, ny) writes the tables: make it outside stream
+ * capture, which such a call rejects with IBPM_ERR_INVALID.  All calls share the array, so
  * calls that overlap on the GPU race.  stream is a cudaStream_t (NULL: default).
  * On error ibpm_noalloc_last_error() gives the message. */
 int ibpm_lap_inv_noalloc(int nx, int ny, const double *b, double *x, void *stream);
