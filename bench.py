@@ -337,39 +337,57 @@ def direct_start_run(ib, device: int, steps: int, warmup: int, npts: int = 101):
                                    "k = 0.55; CG to |r| <= 1e-10", "precision": "fp64"}}
 
 
-def ensemble_report(ib, device: int, seed: int = 2026, n: int = 128, steps: int = 10):
-    """Case-steps/s of n independent FP32 cases (finest grids of {256, 384, 512} x
-    256 cells at h 0.01, 3 levels, seeded cylinders or plates, Re ~ U[50, 300],
-    dt 0.002) stepped together (ibpm_ensemble_advance), against the same cases
-    stepped one after another.  Host-timed between device synchronisations (the
-    cases run on n streams)."""
+def ensemble_report(ib, device: int, pg=None, rank: int = 0, world: int = 1, seed: int = 2026, n: int = 128,
+                    steps: int = 10):
+    """Case-steps/s of one seeded ensemble of n independent FP32 cases (finest
+    grids of {256, 384, 512} x 256 cells at h 0.01, 3 levels, seeded cylinders or
+    plates, Re ~ U[50, 300], dt 0.002) stepped together (ibpm_ensemble_advance),
+    against the same cases stepped one after another.  Under torchrun the cases
+    are sharded over the ranks by cost (no collective on the data path); each
+    rank times its shard with CUDA events on the current stream bracketing the
+    call (which returns after every case's stream has finished), the slowest
+    rank's time counts, and every case's C_D, C_L are gathered at the end."""
     import torch
 
     probs = ib.configs.ensemble_cases(n, seed=seed)
+    costs = [ib.ensemble.case_cost(p) for p in probs]
+    parts = ib.ensemble.shard_cases(costs, world)
+    mine = parts[rank]
+    red = "cuda" if pg else "cpu"
     t0 = time.perf_counter()
-    solvers = [ib.GpuCnabSolver(ib.State(p), precision="fp32", device=device) for p in probs]
+    solvers = [ib.GpuCnabSolver(ib.State(probs[k]), precision="fp32", device=device) for k in mine]
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
     ens = ib.Ensemble(solvers)
+    groups = ens.groups() if hasattr(ens, "groups") else None
     ens.advance_(3, fetch_forces=False)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if pg:
+        pg.barrier()
+    e0.record()
     ens.advance_(steps, fetch_forces=False)
+    e1.record()
     torch.cuda.synchronize()
-    t_conc = time.perf_counter() - t0
-    t0 = time.perf_counter()
+    ms_conc = max_over_ranks(e0.elapsed_time(e1), pg, red)
+    forces = ib.ensemble.gather_case_forces(n, mine, [2 * s.total_force() for s in solvers], pg, red)
+    ens.close()
+    e0.record()
     for s in solvers:
         s.advance_many(steps)
+    e1.record()
     torch.cuda.synchronize()
-    t_seq = time.perf_counter() - t0
-    pts = sum(p.grid.base.n[0] * p.grid.base.n[1] * p.grid.nlevel for p in probs)
-    forces = ens.total_forces()
+    ms_seq = max_over_ranks(e0.elapsed_time(e1), pg, red)
+    pts = sum(costs)
     return {"workload": f"{n} seeded cases (seed {seed}): {{256, 384, 512}} x 256 cells at h 0.01, 3 levels, "
                         "cylinders D ~ U[0.5, 1.5] or plates at AoA ~ U[0, 45] deg, Re ~ U[50, 300], dt 0.002, FP32",
-            "setup_s": t_setup, "steps": steps, "case_steps_per_s": n * steps / t_conc,
-            "grid_point_updates_per_s": pts * steps / t_conc, "ms_per_ensemble_step": 1000.0 * t_conc / steps,
-            "sequential_case_steps_per_s": n * steps / t_seq, "speedup_vs_sequential": t_seq / t_conc,
-            "forces_finite": bool(np.isfinite(forces).all()), "timing": "host clock between device synchronisations"}
+            "ranks": world, "cases_per_rank": [len(p) for p in parts], "batched_groups": groups,
+            "setup_s": t_setup, "steps": steps, "case_steps_per_s": n * steps / (ms_conc / 1000.0),
+            "grid_point_updates_per_s": pts * steps / (ms_conc / 1000.0), "ms_per_ensemble_step": ms_conc / steps,
+            "sequential_case_steps_per_s": n * steps / (ms_seq / 1000.0), "speedup_vs_sequential": ms_seq / ms_conc,
+            "forces_finite": bool(np.isfinite(forces).all()),
+            "timing": "CUDA events on the current stream around the call, slowest rank; cases sharded by cost, "
+                      "forces gathered"}
 
 
 def run_reference(args, world, rank):
@@ -532,7 +550,7 @@ def main():
 
     plate32 = None if args.no_chosen else mixed_precision_plate_report(ib, local)
     learned = None if args.no_learned else warm_start_report(ib, local)
-    ensemble = None if args.no_ensemble else ensemble_report(ib, local, seed=2026 + rank)
+    ensemble = None if args.no_ensemble else ensemble_report(ib, local, pg, rank, world)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

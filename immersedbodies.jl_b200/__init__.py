@@ -16,6 +16,7 @@ from .problem import (CNAB, Bodies, CartesianGrid, Fluid, GridIndices, GridVeloc
                       y_velocity)
 from .solver import AbstractSolver, GpuCnabSolver, advance_, create_solver, getstate, solve, solve_
 from .warmstart import WarmStartNet
+from . import ensemble
 from .ensemble import Ensemble
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -72,3 +72,57 @@ class Ensemble:
     def total_forces(self) -> np.ndarray:
         """boundary_total_force of every case (n x 2)."""
         return np.stack([s.total_force() for s in self.solvers])
+
+
+def case_cost(prob) -> int:
+    """Work of one step of a case, in grid points: every level of the nested
+    grid has the finest level's nx x ny points."""
+    g = prob.grid
+    return int(g.base.n[0]) * int(g.base.n[1]) * int(g.nlevel)
+
+
+def shard_cases(costs: Sequence[int], world: int) -> list:
+    """Partitions cases 0..n-1 over `world` ranks, balanced by cost: the cases
+    are taken in order of decreasing cost (ties by index) and each goes to the
+    rank with the least cost so far (ties by rank).  Deterministic, so every
+    rank computes the same partition without communicating.  Returns one sorted
+    list of case indices per rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda k: (-int(costs[k]), k))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += int(costs[k])
+    return [sorted(p) for p in parts]
+
+
+def gather_case_forces(n_cases: int, local_ids: Sequence[int], local_forces, pg=None, device="cpu") -> np.ndarray:
+    """Per-case total forces of a sharded ensemble, on every rank: each rank
+    contributes the rows of its own cases (n_local x 2) and the rest as zeros,
+    and one sum all-reduce over ranks fills the n_cases x 2 table (every row has
+    exactly one contributor, so the sum is exact).  A third column counts the
+    contributors of each row; a row that is not 1 (a case that no rank or two
+    ranks stepped) raises ValueError.  pg is torch.distributed (or None for one
+    process); device holds the reduction buffer ("cpu" under gloo, "cuda" under
+    NCCL)."""
+    import torch
+
+    t = torch.zeros((n_cases, 3), dtype=torch.float64, device=device)
+    lf = np.asarray(local_forces, dtype=np.float64).reshape(-1, 2)
+    ids = list(local_ids)
+    if len(ids) != lf.shape[0]:
+        raise ValueError("one force row per local case is required")
+    if ids:
+        idx = torch.as_tensor(ids, dtype=torch.long, device=device)
+        t[idx, 0:2] = torch.as_tensor(lf, dtype=torch.float64, device=device)
+        t[idx, 2] = 1.0
+    if pg is not None:
+        pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    out = t.cpu().numpy()
+    if not np.all(out[:, 2] == 1.0):
+        bad = np.nonzero(out[:, 2] != 1.0)[0][:8].tolist()
+        raise ValueError(f"cases without exactly one owning rank: {bad}")
+    return out[:, :2].copy()
