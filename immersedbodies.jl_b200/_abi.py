@@ -84,6 +84,7 @@ EXPORTS = {
     "ibpm_ensemble_advance": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(ibpm_step_params)]),
     "ibpm_ensemble_destroy": (None, [C.c_void_p]),
     "ibpm_ensemble_last_error": (C.c_char_p, [C.c_void_p]),
+    "ibpm_ensemble_groups": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ibpm_net_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
                                   C.POINTER(C.c_void_p)]),
     "ibpm_net_destroy": (None, [C.c_void_p]),

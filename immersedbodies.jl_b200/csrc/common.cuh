@@ -124,6 +124,16 @@ struct Panels {
     int *err;          // err[0]: 0 or 1-based panel index outside the region
 };
 
+// One case of a batched ensemble group, as the multi-case coupling kernels see
+// it: its panels and the buffers of its force solve and regularisation patch.
+struct CaseView {
+    Panels P;
+    double *Ftmp, *part, *Fbt, *fb, *total;
+    const double *Binv;
+    void *patch;  // element type of the group's fields
+    long long patch_stride;
+};
+
 // Regularised flux on the panels' bounding box (compact patch):
 // patch[(i - i0) + pw (j - j0)] for x faces, offset pw*ph for y faces.
 template <class T>

@@ -120,8 +120,7 @@ __global__ void bbox_kernel(Panels P, Grid g) {
 // accumulation order as the reference's sequential loop over panels.
 // f: 2np per batch (x block then y block); patch output per batch.
 template <class T>
-__global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *__restrict__ f, long long fbs,
-                                                        T *__restrict__ patch, long long pbs) {
+__device__ __forceinline__ void reg_patch_tile(const Panels &P, const double *__restrict__ fb, T *__restrict__ out) {
     __shared__ int list[1024];
     __shared__ int warp_cnt[8];
     __shared__ int total;
@@ -130,9 +129,6 @@ __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *
     const int ti0 = i0 + blockIdx.x * kTile, tj0 = j0 + blockIdx.y * kTile;
     if (ti0 > i1 || tj0 > j1) return;
     const int ti1 = min(ti0 + kTile - 1, i1), tj1 = min(tj0 + kTile - 1, j1);
-    const int b = blockIdx.z;
-    const double *fb = f + b * fbs;
-    T *out = patch + b * pbs;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int li = tid % kTile, lj = tid / kTile;
     const int i = ti0 + li, j = tj0 + lj;
@@ -179,6 +175,21 @@ __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *__restrict__ f, long long fbs,
+                                                        T *__restrict__ patch, long long pbs) {
+    const int b = blockIdx.z;
+    reg_patch_tile<T>(P, f + b * fbs, patch + b * pbs);
+}
+
+// reg_patch_kernel for the cases of a batched ensemble group (case = blockIdx.z):
+// each case's E^T F~b onto its own patch.
+template <class T>
+__global__ void __launch_bounds__(256) reg_patch_multi_kernel(const CaseView *__restrict__ tab) {
+    const CaseView &cv = tab[blockIdx.z];
+    reg_patch_tile<T>(cv.P, cv.Fbt, static_cast<T *>(cv.patch));
+}
+
 // regT! (src/coupling.jl:57-69): fb[p, c] = dot(q_c[7x7 at p], w[p, c]) in
 // column-major order.  With add_q0 it is couple_surface_rigid's
 // Ftmp = E (qs + q0) - ub h (src/coupling.jl:239-244).
@@ -187,18 +198,13 @@ __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *
 // support, from 0), so the sum rounds as a sequential dot product.
 constexpr int kRegTWarps = 4;
 template <class T>
-__global__ void __launch_bounds__(32 * kRegTWarps) regT_kernel(Panels P, const T *__restrict__ q, long long qbs,
-                                                                double *__restrict__ out, long long obs, int nbatch,
-                                                                int add_q0, const StepDev *__restrict__ prm, Grid g) {
-    __shared__ double prod[kRegTWarps][49];
+__device__ __forceinline__ void regT_warp(const Panels &P, const T *__restrict__ Q, double *__restrict__ outb,
+                                          int pcomp, int add_q0, const StepDev *__restrict__ prm, const Grid &g,
+                                          double (*prod)[49]) {
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t = blockIdx.x * kRegTWarps + wid;
     const int np = P.np;
-    if (t >= 2 * np * nbatch) return;  // the whole warp leaves together
-    const int b = t / (2 * np), pcomp = t % (2 * np);
     const int c = pcomp / np, p = pcomp % np;
     const long long nu = (long long)(g.nx + 1) * g.ny;
-    const T *Q = q + b * qbs;
     const int i0 = P.pc[2 * p] - 3, j0 = P.pc[2 * p + 1] - 3;
     const double *w = P.w + (long long)(p * 2 + c) * 49;
     for (int k = lane; k < 49; k += 32) {
@@ -213,8 +219,34 @@ __global__ void __launch_bounds__(32 * kRegTWarps) regT_kernel(Panels P, const T
         double s = 0.0;
         for (int k = 0; k < 49; ++k) s += prod[wid][k];
         if (add_q0) s = s - P.ub[c * np + p] * g.h;
-        out[b * obs + c * np + p] = s;
+        outb[c * np + p] = s;
     }
+}
+
+template <class T>
+__global__ void __launch_bounds__(32 * kRegTWarps) regT_kernel(Panels P, const T *__restrict__ q, long long qbs,
+                                                                double *__restrict__ out, long long obs, int nbatch,
+                                                                int add_q0, const StepDev *__restrict__ prm, Grid g) {
+    __shared__ double prod[kRegTWarps][49];
+    const int t = blockIdx.x * kRegTWarps + (threadIdx.x >> 5);
+    const int np = P.np;
+    if (t >= 2 * np * nbatch) return;  // the whole warp leaves together
+    const int b = t / (2 * np), pcomp = t % (2 * np);
+    regT_warp<T>(P, q + b * qbs, out + b * obs, pcomp, add_q0, prm, g, prod);
+}
+
+// couple_surface_rigid's Ftmp = E (qs + q0) - ub h for the cases of a batched
+// ensemble group (case = blockIdx.y; flux stride qbs; callback values prm[case]).
+template <class T>
+__global__ void __launch_bounds__(32 * kRegTWarps) regT_multi_kernel(const CaseView *__restrict__ tab,
+                                                                      const T *__restrict__ q, long long qbs,
+                                                                      const StepDev *__restrict__ prm, Grid g) {
+    __shared__ double prod[kRegTWarps][49];
+    const int cs = blockIdx.y;
+    const CaseView &cv = tab[cs];
+    const int t = blockIdx.x * kRegTWarps + (threadIdx.x >> 5);
+    if (t >= 2 * cv.P.np) return;  // the whole warp leaves together
+    regT_warp<T>(cv.P, q + cs * qbs, cv.Ftmp, t, 1, prm + cs, g, prod);
 }
 
 // _update!(panels, ::MovingRigidBody, t) (src/bodies.jl:12-31) for panels [p0, p1)
@@ -252,6 +284,23 @@ void launch_regT(const Panels &P, const T *q, long long qbs, double *out, long l
     regT_kernel<T><<<(nt + kRegTWarps - 1) / kRegTWarps, 32 * kRegTWarps, 0, st>>>(P, q, qbs, out, obs, nbatch,
                                                                                   add_q0, prm, g);
 }
+template <class T>
+void launch_reg_patch_multi(const CaseView *tab, int ncase, const Grid &g, cudaStream_t st) {
+    const int tiles_x = (g.nx + 1 + kTile - 1) / kTile + 1, tiles_y = (g.ny + 1 + kTile - 1) / kTile + 1;
+    reg_patch_multi_kernel<T><<<dim3(tiles_x, tiles_y, ncase), 256, 0, st>>>(tab);
+}
+template <class T>
+void launch_regT_multi(const CaseView *tab, int ncase, int np_max, const T *q, long long qbs, const StepDev *prm,
+                       const Grid &g, cudaStream_t st) {
+    regT_multi_kernel<T><<<dim3((2 * np_max + kRegTWarps - 1) / kRegTWarps, ncase), 32 * kRegTWarps, 0, st>>>(
+        tab, q, qbs, prm, g);
+}
+template void launch_reg_patch_multi<double>(const CaseView *, int, const Grid &, cudaStream_t);
+template void launch_reg_patch_multi<float>(const CaseView *, int, const Grid &, cudaStream_t);
+template void launch_regT_multi<double>(const CaseView *, int, int, const double *, long long, const StepDev *,
+                                        const Grid &, cudaStream_t);
+template void launch_regT_multi<float>(const CaseView *, int, int, const float *, long long, const StepDev *,
+                                       const Grid &, cudaStream_t);
 template void launch_reg_patch<double>(const Panels &, const double *, long long, double *, long long, int,
                                        const Grid &, cudaStream_t);
 template void launch_reg_patch<float>(const Panels &, const double *, long long, float *, long long, int,

@@ -14,6 +14,20 @@
 
 namespace ibpm {
 
+// Barrier policies of the transforms: the whole block (every group of the block
+// steps through the transform together), or only the TPF threads of the
+// calling thread's group, with hardware barrier 1 + group index (named
+// barriers; groups of one block then run out of step with each other).
+struct CtaSync {
+    static __device__ __forceinline__ void sync() { __syncthreads(); }
+};
+template <int TPF>
+struct GroupSync {
+    static __device__ __forceinline__ void sync() {
+        asm volatile("bar.sync %0, %1;" ::"r"((int)(threadIdx.x / TPF) + 1), "r"(TPF) : "memory");
+    }
+};
+
 // Padded shared-memory index: one spare double2 per 16.
 __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int padded_len(int M) { return (M + 1) + ((M + 1) >> 4) + 1; }
@@ -202,7 +216,7 @@ __host__ __device__ constexpr int write_off(int r) {
 }
 
 // One Stockham stage with compile-time sizes on a padded buffer.
-template <int M, int R, int NS, int TPF, class C>
+template <int M, int R, int NS, int TPF, class C, class S = CtaSync>
 __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t) {
     constexpr int NB = M / R;
     constexpr int K = NB >= TPF ? NB / TPF : 1;  // butterflies per thread
@@ -231,7 +245,7 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t
         }
         DftC<R, C>::run(v[kb]);
     }
-    __syncthreads();
+    S::sync();
 #pragma unroll
     for (int kb = 0; kb < K; ++kb) {
         const int j = t + kb * TPF;
@@ -241,7 +255,7 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t
 #pragma unroll
         for (int r = 0; r < R; ++r) dst[write_off<R, NS>(r)] = v[kb][r];
     }
-    __syncthreads();
+    S::sync();
 }
 
 // The first Stockham stage (stride 1) with the DST pre-twiddle folded into its
@@ -249,7 +263,7 @@ __device__ __forceinline__ void stage_ct(C *buf, const C *__restrict__ tw, int t
 // s = sin(pi min(n, M-n) / M), v_0 = 0 -- the values the separate pre-twiddle
 // pass writes, formed in registers from z_n and its mirror.  buf[0..M] hold z
 // (z_0 = z_M = 0).
-template <int M, int R, int TPF, class C, class T>
+template <int M, int R, int TPF, class C, class T, class S = CtaSync>
 __device__ __forceinline__ void stage_first_pre(C *buf, const T *__restrict__ sn, int t) {
     constexpr int NB = M / R;
     constexpr int K = NB >= TPF ? NB / TPF : 1;
@@ -281,7 +295,7 @@ __device__ __forceinline__ void stage_first_pre(C *buf, const T *__restrict__ sn
         }
         DftC<R, C>::run(v[kb]);
     }
-    __syncthreads();
+    S::sync();
 #pragma unroll
     for (int kb = 0; kb < K; ++kb) {
         const int j = t + kb * TPF;
@@ -290,7 +304,7 @@ __device__ __forceinline__ void stage_first_pre(C *buf, const T *__restrict__ sn
 #pragma unroll
         for (int r = 0; r < R; ++r) dst[write_off<R, 1>(r)] = v[kb][r];
     }
-    __syncthreads();
+    S::sync();
 }
 
 // A Stockham stage with compile-time sizes for any radix and stride: the same
@@ -298,7 +312,7 @@ __device__ __forceinline__ void stage_first_pre(C *buf, const T *__restrict__ sn
 // every element (strides with a factor 3 do not keep the pads at constant
 // offsets).  Butterfly j < M/R takes inputs j + r M/R and writes outputs
 // (j / NS) NS R + j % NS + r NS.
-template <int M, int R, int NS, int TPF, class C>
+template <int M, int R, int NS, int TPF, class C, class S = CtaSync>
 __device__ __forceinline__ void stage_gen(C *buf, const C *__restrict__ tw, int t) {
     constexpr int NB = M / R;
     constexpr int K = (NB + TPF - 1) / TPF;
@@ -322,7 +336,7 @@ __device__ __forceinline__ void stage_gen(C *buf, const C *__restrict__ tw, int 
         }
         DftC<R, C>::run(v[kb]);
     }
-    __syncthreads();
+    S::sync();
 #pragma unroll
     for (int kb = 0; kb < K; ++kb) {
         const int j = t + kb * TPF;
@@ -331,12 +345,12 @@ __device__ __forceinline__ void stage_gen(C *buf, const C *__restrict__ tw, int 
 #pragma unroll
         for (int r = 0; r < R; ++r) buf[pad16(base + r * NS)] = v[kb][r];
     }
-    __syncthreads();
+    S::sync();
 }
 
 // stage_gen's first stage (NS = 1) with the DST pre-twiddle folded into its reads,
 // as stage_first_pre.
-template <int M, int R, int TPF, class C, class T>
+template <int M, int R, int TPF, class C, class T, class S = CtaSync>
 __device__ __forceinline__ void stage_gen_first_pre(C *buf, const T *__restrict__ sn, int t) {
     constexpr int NB = M / R;
     constexpr int K = (NB + TPF - 1) / TPF;
@@ -364,7 +378,7 @@ __device__ __forceinline__ void stage_gen_first_pre(C *buf, const T *__restrict_
         }
         DftC<R, C>::run(v[kb]);
     }
-    __syncthreads();
+    S::sync();
 #pragma unroll
     for (int kb = 0; kb < K; ++kb) {
         const int j = t + kb * TPF;
@@ -372,7 +386,7 @@ __device__ __forceinline__ void stage_gen_first_pre(C *buf, const T *__restrict_
 #pragma unroll
         for (int r = 0; r < R; ++r) buf[pad16(j * R + r)] = v[kb][r];
     }
-    __syncthreads();
+    S::sync();
 }
 
 template <int M, class T, class PL = Pow2Plan<M>>
@@ -392,6 +406,7 @@ struct Pow2Dst {
     // Thread t owns the E = H/TPF consecutive k in [t E, t E + E): a sequential
     // scan of its segment, one warp shuffle scan of the segment totals, and one
     // block barrier for the warp totals.
+    template <class S = CtaSync>
     static __device__ __forceinline__ void post(C *buf, int t, double2 *wt) {
         constexpr int H = M / 2;
         constexpr int E = H / TPF;
@@ -428,7 +443,7 @@ struct Pow2Dst {
         excl.y = __shfl_up_sync(0xffffffffu, incl.y, 1);
         if (lane == 0) excl = make_double2(0.0, 0.0);
         if (NWARP > 1 && lane == 31) wt[w] = incl;
-        __syncthreads();  // all reads of V done; warp totals visible
+        S::sync();  // all reads of V done; warp totals visible
 #pragma unroll
         for (int q = 0; q < NWARP - 1; ++q)
             if (q < w) excl = excl + wt[q];
@@ -442,23 +457,25 @@ struct Pow2Dst {
             buf[0] = Cx<T>::make(0, 0);
             buf[pad16(M)] = Cx<T>::make(0, 0);
         }
-        __syncthreads();
+        S::sync();
     }
 
     // the FFT of the pre-twiddled packed lines, the pre-twiddle folded into stage 1
+    template <class S = CtaSync>
     static __device__ __forceinline__ void fft_pre(C *buf, const C *__restrict__ tw, const T *__restrict__ sn, int t) {
         constexpr int N1 = P::R0, N2 = N1 * P::R1, N3 = N2 * P::R2, N4 = N3 * P::R3;
         static_assert(N4 * P::R4 == M, "plan must factor M");
-        stage_first_pre<M, P::R0, TPF, C, T>(buf, sn, t);
-        stage_ct<M, P::R1, N1, TPF, C>(buf, tw, t);
-        stage_ct<M, P::R2, N2, TPF, C>(buf, tw, t);
-        if constexpr (P::R3 > 1) stage_ct<M, P::R3, N3, TPF, C>(buf, tw, t);
-        if constexpr (P::R4 > 1) stage_ct<M, P::R4, N4, TPF, C>(buf, tw, t);
+        stage_first_pre<M, P::R0, TPF, C, T, S>(buf, sn, t);
+        stage_ct<M, P::R1, N1, TPF, C, S>(buf, tw, t);
+        stage_ct<M, P::R2, N2, TPF, C, S>(buf, tw, t);
+        if constexpr (P::R3 > 1) stage_ct<M, P::R3, N3, TPF, C, S>(buf, tw, t);
+        if constexpr (P::R4 > 1) stage_ct<M, P::R4, N4, TPF, C, S>(buf, tw, t);
     }
 
+    template <class S = CtaSync>
     static __device__ __forceinline__ void dst(C *buf, const PlanT<T> &pl, int t, double2 *wt) {
-        fft_pre(buf, pl.tw, pl.sn, t);
-        post(buf, t, wt);
+        fft_pre<S>(buf, pl.tw, pl.sn, t);
+        post<S>(buf, t, wt);
     }
 };
 
@@ -475,18 +492,20 @@ struct MixDst : Pow2Dst<M, T, PL> {
     using C = typename Base::C;
     using P = PL;
     static constexpr int TPF = P::TPF;
+    template <class S = CtaSync>
     static __device__ __forceinline__ void fft_pre(C *buf, const C *__restrict__ tw, const T *__restrict__ sn, int t) {
         constexpr int N1 = P::R0, N2 = N1 * P::R1, N3 = N2 * P::R2, N4 = N3 * P::R3;
         static_assert(N4 * P::R4 == M, "plan must factor M");
-        stage_gen_first_pre<M, P::R0, TPF, C, T>(buf, sn, t);
-        stage_gen<M, P::R1, N1, TPF, C>(buf, tw, t);
-        stage_gen<M, P::R2, N2, TPF, C>(buf, tw, t);
-        if constexpr (P::R3 > 1) stage_gen<M, P::R3, N3, TPF, C>(buf, tw, t);
-        if constexpr (P::R4 > 1) stage_gen<M, P::R4, N4, TPF, C>(buf, tw, t);
+        stage_gen_first_pre<M, P::R0, TPF, C, T, S>(buf, sn, t);
+        stage_gen<M, P::R1, N1, TPF, C, S>(buf, tw, t);
+        stage_gen<M, P::R2, N2, TPF, C, S>(buf, tw, t);
+        if constexpr (P::R3 > 1) stage_gen<M, P::R3, N3, TPF, C, S>(buf, tw, t);
+        if constexpr (P::R4 > 1) stage_gen<M, P::R4, N4, TPF, C, S>(buf, tw, t);
     }
+    template <class S = CtaSync>
     static __device__ __forceinline__ void dst(C *buf, const PlanT<T> &pl, int t, double2 *wt) {
-        fft_pre(buf, pl.tw, pl.sn, t);
-        Base::post(buf, t, wt);
+        fft_pre<S>(buf, pl.tw, pl.sn, t);
+        Base::template post<S>(buf, t, wt);
     }
 };
 

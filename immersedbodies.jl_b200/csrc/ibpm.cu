@@ -20,6 +20,8 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <initializer_list>
+#include <memory>
 #include <vector>
 
 #include "../../include/ibpm_b200.h"
@@ -363,25 +365,27 @@ struct Engine final : ibpm_handle {
     // Dispatch on the transform length: compile-time transforms for
     // M in {256, 384, 512, 1024}, the runtime mixed-radix one otherwise.
     template <class D, class In, class Out>
-    void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch, const int *rows, int zero_outside) {
+    void xpass_t(const PlanT<typename D::Real> &pl, In in, Out out, int nbatch, const int *rows, int zero_outside,
+                 int rows_stride) {
         const int pairs = (ny - 1 + 1) / 2;
         const dim3 grid((pairs + kNG - 1) / kNG, nbatch);
         const size_t sm = pass_smem<D>(pl.M, kNG, kNG);
-        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, pl, ny - 1, rows, zero_outside);
+        xpass_kernel<D, kNG, In, Out><<<grid, kNG * D::TPF, sm, st>>>(in, out, pl, ny - 1, rows, zero_outside,
+                                                                       rows_stride);
     }
     // X pass with transforms of element type R (the engine's T, or double for
     // the FP32 engine's FP64 level-1 solve); In/Out convert at the boundary.
-    // rows, zero_outside: see xpass_kernel (rows null: every row).
+    // rows, zero_outside, rows_stride: see xpass_kernel (rows null: every row).
     template <class R = T, class In, class Out>
-    void xpass(In in, Out out, int nbatch, const int *rows = nullptr, int zero_outside = 0) {
+    void xpass(In in, Out out, int nbatch, const int *rows = nullptr, int zero_outside = 0, int rows_stride = 0) {
         const PlanT<R> &pl = plan_x<R>();
         const int pe = prof_begin();
         switch (pl.M) {
-            case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch, rows, zero_outside); break;
-            case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch, rows, zero_outside); break;
-            case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch, rows, zero_outside); break;
-            case 384: xpass_t<MixDst<384, R>>(pl, in, out, nbatch, rows, zero_outside); break;
-            default: xpass_t<GenericDst<R>>(pl, in, out, nbatch, rows, zero_outside); break;
+            case 1024: xpass_t<Pow2Dst<1024, R>>(pl, in, out, nbatch, rows, zero_outside, rows_stride); break;
+            case 512: xpass_t<Pow2Dst<512, R>>(pl, in, out, nbatch, rows, zero_outside, rows_stride); break;
+            case 256: xpass_t<Pow2Dst<256, R>>(pl, in, out, nbatch, rows, zero_outside, rows_stride); break;
+            case 384: xpass_t<MixDst<384, R>>(pl, in, out, nbatch, rows, zero_outside, rows_stride); break;
+            default: xpass_t<GenericDst<R>>(pl, in, out, nbatch, rows, zero_outside, rows_stride); break;
         }
         check_launch();
         prof_end(pe, IBPM_KCLASS_XPASS, 2.0 * sizeof(R) * (double)ng * nbatch);
@@ -442,18 +446,20 @@ struct Engine final : ibpm_handle {
     }
     double *psi1_hi = nullptr, *qs1_hi = nullptr, *t1_hi = nullptr, *t2_hi = nullptr;
     // Merged trial solve over all L levels: Gamma_new = Ainv(A Gamma + rest)
+    // nb batches of ng (L for one case; cases x L for an ensemble group, whose
+    // per-batch coefficients dt / (2 Re hc^2) come from ctab)
     template <class D>
-    void trial_t(const T *Gold, const T *rest_, T *Gnew) {
+    void trial_t(const T *Gold, const T *rest_, T *Gnew, int nb, const double *ctab) {
         {
-            const dim3 grid((ny - 1 + kNG - 1) / kNG, L);
+            const dim3 grid((ny - 1 + kNG - 1) / kNG, nb);
             const size_t sm = pass_smem<D>(plx.M, kNG, kNG);
             const int pe = prof_begin();
             xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1, t2, ng, nx - 1, plx, ny - 1);
             check_launch();
-            prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(T) * (double)ng * L);
+            prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(T) * (double)ng * nb);
         }
         {
-            const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), L);
+            const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nb);
             const size_t sm = pass_smem<D>(ply.M, 2 * kNG, kNG);
             // the cap must cover the largest M this instantiation serves (kMaxM); the
             // attribute is per device
@@ -464,22 +470,24 @@ struct Engine final : ibpm_handle {
                 attr_devices.fetch_or(device_bit());
             }
             const int pe = prof_begin();
-            ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1, t2, rhs, ng, nx - 1, ply,
-                                                                       mult(MULT_AIMPL, 1, 1));
+            Mult m = mult(MULT_AIMPL, 1, 1);
+            m.coef_tab = ctab;
+            ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1, t2, rhs, ng, nx - 1, ply, m);
             check_launch();
-            prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(T) * (double)ng * L);
+            prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(T) * (double)ng * nb);
         }
-        xpass(in_plain(rhs, ng), out_plain(Gnew, ng), L);
+        xpass(in_plain(rhs, ng), out_plain(Gnew, ng), nb);
     }
-    void trial(const T *Gold, const T *rest_, T *Gnew) {
+    void trial(const T *Gold, const T *rest_, T *Gnew, int nb = 0, const double *ctab = nullptr) {
+        if (nb == 0) nb = L;
         if (plx.M == 1024 && ply.M == 1024)
-            trial_t<Pow2Dst<1024, T>>(Gold, rest_, Gnew);
+            trial_t<Pow2Dst<1024, T>>(Gold, rest_, Gnew, nb, ctab);
         else if (plx.M == 512 && ply.M == 512)
-            trial_t<Pow2Dst<512, T>>(Gold, rest_, Gnew);
+            trial_t<Pow2Dst<512, T>>(Gold, rest_, Gnew, nb, ctab);
         else if (plx.M == 256 && ply.M == 256)
-            trial_t<Pow2Dst<256, T>>(Gold, rest_, Gnew);
+            trial_t<Pow2Dst<256, T>>(Gold, rest_, Gnew, nb, ctab);
         else
-            trial_t<GenericDst<T>>(Gold, rest_, Gnew);
+            trial_t<GenericDst<T>>(Gold, rest_, Gnew, nb, ctab);
     }
 
     Mult mult(int mode, int lev0, int levstep) const {
@@ -493,6 +501,7 @@ struct Engine final : ibpm_handle {
         m.dt = g.dt;
         m.lev0 = lev0;
         m.levstep = levstep;
+        m.coef_tab = nullptr;
         return m;
     }
     InPlain<T> in_plain(const T *p, long long bs) const { return InPlain<T>{p, bs, nx - 1}; }
@@ -518,17 +527,18 @@ struct Engine final : ibpm_handle {
             T *Gl = Gm + (lev - 1) * ng;
             T *Pl = psi_ + (lev - 1) * ng;
             if (lev == 1 && hi1) {
-                // level 1 in FP64 from the FP32 coarser levels: psi1_hi and qs1_hi (x E)
+                // level 1 in FP64 from the FP32 coarser levels: psi1_hi and qs1_hi (x E),
+                // batch strides ng and nq
                 const T *coarse = L > 1 ? psi_ + ng : nullptr;
                 if (coarse)
-                    xpass<double>(InBC<T>{Gl, coarse, bs, bs, g}, OutPlain<double>{t1_hi, ng, nx - 1}, 1);
+                    xpass<double>(InBC<T>{Gl, coarse, bs, bs, g}, OutPlain<double>{t1_hi, ng, nx - 1}, nbatch);
                 else
-                    xpass<double>(in_plain(Gl, bs), OutPlain<double>{t1_hi, ng, nx - 1}, 1);
-                ypass<double>(t1_hi, t2_hi, ng, 1, mult(MULT_LAPINV, 1, 0));
-                xpass<double>(InPlain<double>{t2_hi, ng, nx - 1}, OutPlain<double>{psi1_hi, ng, nx - 1}, 1);
+                    xpass<double>(in_plain(Gl, bs), OutPlain<double>{t1_hi, ng, nx - 1}, nbatch);
+                ypass<double>(t1_hi, t2_hi, ng, nbatch, mult(MULT_LAPINV, 1, 0));
+                xpass<double>(InPlain<double>{t2_hi, ng, nx - 1}, OutPlain<double>{psi1_hi, ng, nx - 1}, nbatch);
                 const dim3 blk(64, 4);
-                const dim3 grd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, 1);
-                curl_kernel<double, double, T><<<grd, blk, 0, st>>>(qs1_hi, 0, psi1_hi, 0, coarse, 0, g);
+                const dim3 grd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, nbatch);
+                curl_kernel<double, double, T><<<grd, blk, 0, st>>>(qs1_hi, nq, psi1_hi, ng, coarse, bs, g);
                 check_launch();
                 continue;
             }
@@ -1781,6 +1791,346 @@ void Engine<T>::diag_reg(const double *f, double *gamma1, const double *q1, doub
 }
 
 // ---------------------------------------------------------------------------
+// Ensembles: cases of one shape stepped as one batch
+// ---------------------------------------------------------------------------
+
+// Static-body, static-grid cases of one precision with equal nx, ny, levels,
+// grid step and time step (they may differ in Reynolds number, domain origin,
+// bodies and freestream) are stepped together: their fields are stacked
+// case-major in one allocation (batch b = case L + level - 1), and every line
+// pass, the nonlinear term, the curls and the coarsening run as one launch over
+// all cases, and so does the coupling (E, B^-1, E^T), each case on its own
+// panels through a device table of CaseViews.  A group step is one CUDA graph.
+// Each case's per-element arithmetic is that of stepping it alone, so its
+// results are the same bits.  While grouped, each case's engine points at its
+// slot of the stacked fields (a single advance of one case still works); the
+// ensemble's destruction copies every case back into buffers of its own.
+template <class T>
+struct CaseGroup {
+    std::vector<Engine<T> *> cs;
+    Engine<T> *e0 = nullptr;  // the first case: shape, tables, launch helpers
+    int C = 0, L = 0;
+    long long ng = 0, nq = 0;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    T *q = nullptr, *psi = nullptr, *G[2] = {nullptr, nullptr}, *nl[2] = {nullptr, nullptr};
+    T *t1 = nullptr, *t2 = nullptr, *rhs = nullptr, *rest = nullptr, *qs1 = nullptr;
+    double *t1_hi = nullptr, *t2_hi = nullptr, *psi1_hi = nullptr, *qs1_hi = nullptr;
+    double *coef_all = nullptr, *coef_lev1 = nullptr, *re_tab = nullptr;
+    StepDev *prm_tab = nullptr;
+    CaseView *views = nullptr;  // each case's panels and force-solve buffers (device)
+    int *bbox_tab = nullptr;    // each case's face window, 4 ints per case (device)
+    int np_max = 0;
+    static constexpr int kStage = 8;
+    StepDev *stage_h[kStage] = {};
+    cudaEvent_t stage_ev[kStage] = {};
+    bool stage_used[kStage] = {};
+    int stage_next = 0;
+    int gc = 0, nc = 0;
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    std::vector<void *> mem;
+
+    template <class U>
+    U *alloc(size_t n) {
+        void *p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(U)) != cudaSuccess) {
+            (void)cudaGetLastError();
+            throw ApiError{IBPM_ERR_NOMEM, "cudaMalloc of an ensemble group's fields failed"};
+        }
+        mem.push_back(p);
+        return static_cast<U *>(p);
+    }
+
+    // true when e can join a group led by f
+    static bool compatible(const Engine<T> *f, const Engine<T> *e) {
+        return e->device == f->device && e->nx == f->nx && e->ny == f->ny && e->L == f->L && e->g.h == f->g.h &&
+               e->g.dt == f->g.dt && e->hi_level1 == f->hi_level1;
+    }
+    static bool eligible(const Engine<T> *e) {
+        return e->static_bodies && !e->g.grid_moving && e->Binv != nullptr && !e->prof;
+    }
+
+    void bind(const std::vector<Engine<T> *> &cases) {
+        cs = cases;
+        C = (int)cs.size();
+        e0 = cs[0];
+        L = e0->L;
+        ng = e0->ng;
+        nq = e0->nq;
+        device = e0->device;
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        for (int k = 0; k < kStage; ++k) {
+            CK(cudaMallocHost(&stage_h[k], sizeof(StepDev) * C));
+            CK(cudaEventCreateWithFlags(&stage_ev[k], cudaEventDisableTiming));
+        }
+        const size_t ngL = (size_t)(ng * L), nqL = (size_t)(nq * L);
+        q = alloc<T>(nqL * C);
+        psi = alloc<T>(ngL * C);
+        G[0] = alloc<T>(ngL * C);
+        G[1] = alloc<T>(ngL * C);
+        nl[0] = alloc<T>(ngL * C);
+        nl[1] = alloc<T>(ngL * C);
+        t1 = alloc<T>(ngL * C);
+        t2 = alloc<T>(ngL * C);
+        rhs = alloc<T>(ngL * C);
+        rest = alloc<T>(ngL * C);
+        qs1 = alloc<T>((size_t)nq * C);
+        if (e0->hi_level1) {
+            t1_hi = alloc<double>((size_t)ng * C);
+            t2_hi = alloc<double>((size_t)ng * C);
+            psi1_hi = alloc<double>((size_t)ng * C);
+            qs1_hi = alloc<double>((size_t)nq * C);
+        }
+        prm_tab = alloc<StepDev>(C);
+        // dt / (2 Re hc^2) per (case, level), as Mult::coef forms it on the device
+        std::vector<double> ca((size_t)C * L), c1(C), re(C);
+        for (int c = 0; c < C; ++c) {
+            const Grid &g = cs[c]->g;
+            re[c] = g.Re;
+            for (int lev = 1; lev <= L; ++lev) {
+                const double hc = ldexp(g.h, lev - 1);
+                ca[(size_t)c * L + lev - 1] = g.dt / (2 * g.Re * (hc * hc));
+            }
+            c1[c] = ca[(size_t)c * L];
+        }
+        coef_all = alloc<double>(ca.size());
+        coef_lev1 = alloc<double>(C);
+        re_tab = alloc<double>(C);
+        CK(cudaMemcpyAsync(coef_all, ca.data(), sizeof(double) * ca.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(coef_lev1, c1.data(), sizeof(double) * C, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(re_tab, re.data(), sizeof(double) * C, cudaMemcpyHostToDevice, st));
+        std::vector<CaseView> hv(C);
+        views = alloc<CaseView>(C);
+        bbox_tab = alloc<int>(4 * (size_t)C);
+        for (int c = 0; c < C; ++c) {
+            Engine<T> &ec = *cs[c];
+            CK(cudaStreamSynchronize(ec.st));
+            hv[c] = CaseView{ec.P, ec.Ftmp, ec.part, ec.Fbt, ec.fb, ec.total, ec.Binv, ec.patch, ec.patch_stride};
+            np_max = std::max(np_max, ec.np);
+            CK(cudaMemcpyAsync(bbox_tab + 4 * c, ec.P.bbox, sizeof(int) * 4, cudaMemcpyDeviceToDevice, st));
+        }
+        CK(cudaMemcpyAsync(views, hv.data(), sizeof(CaseView) * C, cudaMemcpyHostToDevice, st));
+        // move every case's state into its slot and point the case there
+        for (int c = 0; c < C; ++c) {
+            Engine<T> &e = *cs[c];
+            const size_t og = ngL * c, oq = nqL * c;
+            CK(cudaMemcpyAsync(q + oq, e.q, sizeof(T) * nqL, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(psi + og, e.psi, sizeof(T) * ngL, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(G[0] + og, e.G[e.gc], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(G[1] + og, e.G[1 - e.gc], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(nl[0] + og, e.nl[e.nc], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(nl[1] + og, e.nl[1 - e.nc], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(prm_tab + c, e.prm, sizeof(StepDev), cudaMemcpyDeviceToDevice, st));
+        }
+        CK(cudaStreamSynchronize(st));
+        for (int c = 0; c < C; ++c) {
+            Engine<T> &e = *cs[c];
+            e.drop_graphs();
+            T *own[6] = {e.q, e.psi, e.G[0], e.G[1], e.nl[0], e.nl[1]};
+            for (int k = 0; k < 6; ++k) e.dfree(own[k]);
+            const size_t og = ngL * c, oq = nqL * c;
+            e.q = q + oq;
+            e.psi = psi + og;
+            e.G[0] = G[0] + og;
+            e.G[1] = G[1] + og;
+            e.nl[0] = nl[0] + og;
+            e.nl[1] = nl[1] + og;
+            e.gc = 0;
+            e.nc = 0;
+        }
+    }
+
+    // copies every case back into buffers of its own (before the group's memory goes)
+    void unbind() {
+        if (cs.empty()) return;
+        CK(cudaSetDevice(device));
+        CK(cudaStreamSynchronize(st));
+        const size_t ngL = (size_t)(ng * L), nqL = (size_t)(nq * L);
+        for (int c = 0; c < C; ++c) {
+            Engine<T> &e = *cs[c];
+            CK(cudaStreamSynchronize(e.st));
+            e.drop_graphs();
+            T *nq_ = e.template dalloc<T>(nqL), *np_ = e.template dalloc<T>(ngL);
+            T *g0 = e.template dalloc<T>(ngL), *g1 = e.template dalloc<T>(ngL);
+            T *n0 = e.template dalloc<T>(ngL), *n1 = e.template dalloc<T>(ngL);
+            CK(cudaMemcpyAsync(nq_, e.q, sizeof(T) * nqL, cudaMemcpyDeviceToDevice, e.st));
+            CK(cudaMemcpyAsync(np_, e.psi, sizeof(T) * ngL, cudaMemcpyDeviceToDevice, e.st));
+            CK(cudaMemcpyAsync(g0, e.G[0], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, e.st));
+            CK(cudaMemcpyAsync(g1, e.G[1], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, e.st));
+            CK(cudaMemcpyAsync(n0, e.nl[0], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, e.st));
+            CK(cudaMemcpyAsync(n1, e.nl[1], sizeof(T) * ngL, cudaMemcpyDeviceToDevice, e.st));
+            CK(cudaStreamSynchronize(e.st));
+            e.q = nq_;
+            e.psi = np_;
+            e.G[0] = g0;
+            e.G[1] = g1;
+            e.nl[0] = n0;
+            e.nl[1] = n1;
+        }
+        cs.clear();
+    }
+
+    ~CaseGroup() {
+        try {
+            unbind();
+        } catch (...) {
+        }
+        for (int p = 0; p < 2; ++p) {
+            if (exec[p]) cudaGraphExecDestroy(exec[p]);
+            if (graph[p]) cudaGraphDestroy(graph[p]);
+        }
+        for (void *p : mem) cudaFree(p);
+        for (int k = 0; k < kStage; ++k) {
+            if (stage_h[k]) cudaFreeHost(stage_h[k]);
+            if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
+        }
+        if (st) cudaStreamDestroy(st);
+    }
+
+    // Lends e0's launch helpers the group's stream and scratch for one call.
+    struct Borrow {
+        Engine<T> &e;
+        cudaStream_t st;
+        T *t1, *t2, *rhs;
+        double *t1_hi, *t2_hi, *psi1_hi, *qs1_hi;
+        Borrow(Engine<T> &e_, CaseGroup &gr) : e(e_) {
+            st = e.st;
+            t1 = e.t1;
+            t2 = e.t2;
+            rhs = e.rhs;
+            t1_hi = e.t1_hi;
+            t2_hi = e.t2_hi;
+            psi1_hi = e.psi1_hi;
+            qs1_hi = e.qs1_hi;
+            e.st = gr.st;
+            e.t1 = gr.t1;
+            e.t2 = gr.t2;
+            e.rhs = gr.rhs;
+            e.t1_hi = gr.t1_hi;
+            e.t2_hi = gr.t2_hi;
+            e.psi1_hi = gr.psi1_hi;
+            e.qs1_hi = gr.qs1_hi;
+        }
+        ~Borrow() {
+            e.st = st;
+            e.t1 = t1;
+            e.t2 = t2;
+            e.rhs = rhs;
+            e.t1_hi = t1_hi;
+            e.t2_hi = t2_hi;
+            e.psi1_hi = psi1_hi;
+            e.qs1_hi = qs1_hi;
+        }
+    };
+
+    // advance! of every case (src/solver.jl:155-190), batched; e0's helpers launch
+    // on the group stream (Borrow)
+    void step_body() {
+        Engine<T> &e = *e0;
+        Borrow bw(e, *this);
+        T *Gold = G[gc], *Gnew = G[1 - gc];
+        T *N1 = nl[nc], *N2 = nl[1 - nc];
+        const long long bsG = ng * L, bsQ = nq * L;
+        {
+            NonlinArgs<T> a{q, Gold, N1, N2, rest, prm_tab, e.g, re_tab, 1};
+            const dim3 blk(kNlTX, kNlBY), grd((e.nx - 1 + kNlTX - 1) / kNlTX, (e.ny - 1 + kNlTY - 1) / kNlTY, C * L);
+            nonlinear_kernel<<<grd, blk, 0, st>>>(a);
+            e.check_launch();
+        }
+        e.trial(Gold, rest, Gnew, C * L, coef_all);
+        nc = 1 - nc;
+        e.vort2flux(psi, e.hi_level1 ? nullptr : qs1, Gnew, bsG, nq, C, false, e.hi_level1, nullptr);
+        // per case, one launch over all cases each: E qs, F~b = B^-1 Ftmp,
+        // update_vars!, E^T F~b and the X pass of its rot (zero outside each case's window)
+        if (e.hi_level1)
+            launch_regT_multi<double>(views, C, np_max, qs1_hi, nq, prm_tab, e.g, st);
+        else
+            launch_regT_multi<T>(views, C, np_max, qs1, nq, prm_tab, e.g, st);
+        e.check_launch();
+        const int nchunk = (2 * np_max + 63) / 64;
+        binv_gemv_multi_kernel<<<dim3(nchunk, nchunk, C), 256, 0, st>>>(views);
+        e.check_launch();
+        binv_reduce_multi_kernel<<<C, 1024, 0, st>>>(views, e.g.h, e.g.dt);
+        e.check_launch();
+        launch_reg_patch_multi<T>(views, C, e.g, st);
+        e.check_launch();
+        e.xpass(InRegRotTab<T>{views}, e.out_plain(t1, ng), C, bbox_tab, 1, 4);
+        // project_circ's solve at level 1 of every case, then vort2flux!
+        Mult m = e.mult(MULT_AIMPL, 1, 0);
+        m.coef_tab = coef_lev1;
+        e.ypass(t1, t2, ng, C, m);
+        e.xpass(e.in_plain(t2, ng), OutSub<T>{Gnew, bsG, e.nx - 1}, C);
+        e.vort2flux(psi, q, Gnew, bsG, bsQ, C, true);
+        gc = 1 - gc;
+    }
+
+    // one step of every case: this step's callback values, then the group's graph
+    void step(const std::vector<const ibpm_step_params *> &prm) {
+        CK(cudaSetDevice(device));
+        const int k = stage_next;
+        stage_next = (stage_next + 1) % kStage;
+        if (stage_used[k]) CK(cudaEventSynchronize(stage_ev[k]));
+        stage_used[k] = true;
+        for (int c = 0; c < C; ++c) {
+            StepDev &d = stage_h[k][c];
+            d.fs[0] = prm[c]->freestream[0];
+            d.fs[1] = prm[c]->freestream[1];
+            for (int j = 0; j < 6; ++j) d.gm[j] = prm[c]->grid_motion[j];
+        }
+        CK(cudaMemcpyAsync(prm_tab, stage_h[k], sizeof(StepDev) * C, cudaMemcpyHostToDevice, st));
+        CK(cudaEventRecord(stage_ev[k], st));
+        const int p = gc;
+        if (!exec[p]) {
+            const int gc0 = gc, nc0 = nc;
+            const long long l0 = e0->launches;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            try {
+                step_body();
+            } catch (...) {
+                cudaGraph_t gdrop = nullptr;
+                cudaStreamEndCapture(st, &gdrop);
+                if (gdrop) cudaGraphDestroy(gdrop);
+                (void)cudaGetLastError();
+                gc = gc0;
+                nc = nc0;
+                e0->launches = l0;
+                throw;
+            }
+            CK(cudaStreamEndCapture(st, &graph[p]));
+            CK(cudaGraphInstantiate(&exec[p], graph[p], 0));
+            gc = gc0;
+            nc = nc0;
+            e0->launches = l0;
+        }
+        CK(cudaGraphLaunch(exec[p], st));
+        gc = 1 - gc;
+        nc = 1 - nc;
+        for (int c = 0; c < C; ++c) {
+            Engine<T> &e = *cs[c];
+            ++e.index;
+            e.gc = gc;
+            e.nc = nc;
+            e.q0_zero = false;
+            e.q0_from_user = false;
+            e.last_cg_iters = 0;
+            e.fs_last[0] = prm[c]->freestream[0];
+            e.fs_last[1] = prm[c]->freestream[1];
+            for (int j = 0; j < 6; ++j) e.gm_last[j] = prm[c]->grid_motion[j];
+        }
+    }
+
+    // waits for the group's steps; each case's own parameter block gets the last step's values
+    void finish() {
+        CK(cudaSetDevice(device));
+        for (int c = 0; c < C; ++c)
+            CK(cudaMemcpyAsync(cs[c]->prm, prm_tab + c, sizeof(StepDev), cudaMemcpyDeviceToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+};
+
+// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 
@@ -1933,43 +2283,138 @@ int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params)
 struct ibpm_ensemble {
     std::vector<ibpm_handle *> cases;
     std::string last_error;
+    std::vector<std::unique_ptr<CaseGroup<double>>> g64;
+    std::vector<std::unique_ptr<CaseGroup<float>>> g32;
+    std::vector<std::vector<int>> members64, members32;  // case indices of each group
+    std::vector<int> alone;                              // cases stepped on their own streams
+    ~ibpm_ensemble() {
+        g64.clear();  // each group copies its cases back into buffers of their own
+        g32.clear();
+    }
 };
+
+}  // extern "C"
+
+namespace {
+// Groups the eligible cases of one precision by shape (groups of one stay alone).
+template <class T>
+void form_groups(ibpm_ensemble *e, std::vector<std::unique_ptr<CaseGroup<T>>> &groups,
+                 std::vector<std::vector<int>> &members, std::vector<bool> &taken) {
+    std::vector<std::vector<int>> lists;
+    for (int c = 0; c < (int)e->cases.size(); ++c) {
+        Engine<T> *x = dynamic_cast<Engine<T> *>(e->cases[c]);
+        if (!x || !CaseGroup<T>::eligible(x)) continue;
+        bool placed = false;
+        for (auto &l : lists)
+            if (CaseGroup<T>::compatible(dynamic_cast<Engine<T> *>(e->cases[l[0]]), x)) {
+                l.push_back(c);
+                placed = true;
+                break;
+            }
+        if (!placed) lists.push_back({c});
+    }
+    for (auto &l : lists) {
+        if (l.size() < 2) continue;
+        std::vector<Engine<T> *> es;
+        for (int c : l) es.push_back(dynamic_cast<Engine<T> *>(e->cases[c]));
+        std::unique_ptr<CaseGroup<T>> gr(new CaseGroup<T>());
+        gr->bind(es);
+        groups.push_back(std::move(gr));
+        members.push_back(l);
+        for (int c : l) taken[c] = true;
+    }
+}
+
+template <class T>
+void step_groups(ibpm_ensemble *e, std::vector<std::unique_ptr<CaseGroup<T>>> &groups,
+                 const std::vector<std::vector<int>> &members, const ibpm_step_params *params, int64_t k) {
+    const int64_t n = (int64_t)e->cases.size();
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        std::vector<const ibpm_step_params *> prm;
+        for (int c : members[gi]) prm.push_back(&params[k * n + c]);
+        groups[gi]->step(prm);
+    }
+}
+}  // namespace
+
+extern "C" {
 
 int ibpm_ensemble_create(ibpm_handle *const *cases, int32_t n, ibpm_ensemble **out) {
     if (!out) return IBPM_ERR_INVALID;
     *out = nullptr;
     if (n < 1 || !cases) return IBPM_ERR_INVALID;
-    for (int32_t c = 0; c < n; ++c)
+    for (int32_t c = 0; c < n; ++c) {
         if (!cases[c]) return IBPM_ERR_INVALID;
+        for (int32_t d = 0; d < c; ++d)
+            if (cases[d] == cases[c]) return IBPM_ERR_INVALID;  // a case may appear once
+    }
     ibpm_ensemble *e = new ibpm_ensemble;
     e->cases.assign(cases, cases + n);
+    bool batch = true;
+    if (const char *v = getenv("IBPM_ENSEMBLE_BATCH")) batch = v[0] != '0';
+    std::vector<bool> taken(n, false);
+    const int rc = guarded(nullptr, [&] {
+        if (batch) {
+            form_groups<double>(e, e->g64, e->members64, taken);
+            form_groups<float>(e, e->g32, e->members32, taken);
+        }
+    });
+    if (rc != IBPM_OK) {
+        g_create_error = "grouping the ensemble's cases failed";
+        delete e;
+        return rc;
+    }
+    for (int c = 0; c < n; ++c)
+        if (!taken[c]) e->alone.push_back(c);
     *out = e;
     return IBPM_OK;
 }
 
 void ibpm_ensemble_destroy(ibpm_ensemble *e) { delete e; }
 
-// Round-robin over the cases: each step of every case is enqueued on that case's
-// own stream before any is waited for, so the cases' step graphs run side by
-// side on the GPU.
+// Each step: every group's batched step graph, and each remaining case's step on
+// its own stream, all enqueued before any is waited for.
 int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_params *params) {
     if (!e || nsteps < 0 || (nsteps > 0 && !params)) return IBPM_ERR_INVALID;
     const int64_t n = (int64_t)e->cases.size();
-    for (int64_t k = 0; k < nsteps; ++k)
-        for (int64_t c = 0; c < n; ++c) {
+    auto finish_all = [&] {
+        for (auto &g : e->g64) guarded(nullptr, [&] { g->finish(); });
+        for (auto &g : e->g32) guarded(nullptr, [&] { g->finish(); });
+        for (int c : e->alone) guarded(e->cases[c], [&] { e->cases[c]->finish_steps(); });
+    };
+    for (int64_t k = 0; k < nsteps; ++k) {
+        int rc = guarded(nullptr, [&] {
+            step_groups<double>(e, e->g64, e->members64, params, k);
+            step_groups<float>(e, e->g32, e->members32, params, k);
+        });
+        if (rc != IBPM_OK) {
+            e->last_error = "batched group: step failed";
+            finish_all();
+            return rc;
+        }
+        for (int c : e->alone) {
             ibpm_handle *h = e->cases[c];
-            const int rc = guarded(h, [&] { h->enqueue_step(params[k * n + c]); });
+            rc = guarded(h, [&] { h->enqueue_step(params[k * n + c]); });
             if (rc != IBPM_OK) {
                 e->last_error = "case " + std::to_string(c) + ": " + h->last_error;
-                for (ibpm_handle *o : e->cases) guarded(o, [&] { o->finish_steps(); });
+                finish_all();
                 return rc;
             }
         }
+    }
+    int rc = guarded(nullptr, [&] {
+        for (auto &g : e->g64) g->finish();
+        for (auto &g : e->g32) g->finish();
+    });
+    if (rc != IBPM_OK) {
+        e->last_error = "batched group: synchronisation failed";
+        return rc;
+    }
     bool maxiter = false;
-    for (int64_t c = 0; c < n; ++c) {
+    for (int c : e->alone) {
         ibpm_handle *h = e->cases[c];
         bool m = false;
-        const int rc = guarded(h, [&] { m = h->finish_steps(); });
+        rc = guarded(h, [&] { m = h->finish_steps(); });
         if (rc != IBPM_OK) {
             e->last_error = "case " + std::to_string(c) + ": " + h->last_error;
             return rc;
@@ -1980,6 +2425,16 @@ int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_para
         e->last_error = "CG reached maxiter";
         return IBPM_WARN_CG_MAXITER;
     }
+    return IBPM_OK;
+}
+
+int ibpm_ensemble_groups(const ibpm_ensemble *e, int32_t *ngroups, int32_t *nbatched) {
+    if (!e) return IBPM_ERR_INVALID;
+    int32_t ng = 0, nb = 0;
+    for (auto &m : e->members64) ++ng, nb += (int32_t)m.size();
+    for (auto &m : e->members32) ++ng, nb += (int32_t)m.size();
+    if (ngroups) *ngroups = ng;
+    if (nbatched) *nbatched = nb;
     return IBPM_OK;
 }
 

@@ -80,6 +80,18 @@ struct InRegRot {
     }
 };
 
+// Prologue rot!(Gamma, reg!(q, f)) of the cases of a batched ensemble group:
+// batch b reads case b's patch (zero outside its bounding box).
+template <class T>
+struct InRegRotTab {
+    const CaseView *tab;
+    __device__ __forceinline__ double operator()(int b, int I, int J) const {
+        const CaseView &cv = tab[b];
+        const Patch<T> pt{static_cast<const T *>(cv.patch), cv.P.bbox, 0};
+        return (pt.get(0, 0, I + 1, J) - pt.get(0, 0, I + 1, J + 1)) + (pt.get(0, 1, I + 1, J + 1) - pt.get(0, 1, I, J + 1));
+    }
+};
+
 // Epilogue: plain store
 template <class T>
 struct OutPlain {
@@ -124,9 +136,11 @@ struct Mult {
     double scale;       // 1 / (4 nx ny)
     double h, Re, dt;
     int lev0, levstep;  // level of batch b: lev0 + b * levstep
+    const double *coef_tab;  // device, may be null: c of batch b (cases of an ensemble differ in Re)
     // c = dt / (2 Re hc^2) of the batch's level; the reference's (lam dt) / (2 Re hc^2)
     // becomes lam c (within one rounding), which leaves one division per element.
     __device__ __forceinline__ double coef(int b) const {
+        if (coef_tab) return coef_tab[b];
         const int lev = lev0 + b * levstep;
         const double hc = ldexp(h, lev - 1);
         return dt / (2 * Re * (hc * hc));
@@ -144,7 +158,8 @@ struct Mult {
 
 // X pass: DST along x of rows (ja, jb) = (2p+1, 2p+2) of each batch field.
 // D is the line transform (Pow2Dst<M> or GenericDst); NG line pairs per block.
-// rows (device, may be null): the body's face window i0, i1, j0, j1.  A block
+// rows (device, may be null): the body's face window i0, i1, j0, j1 (batch b's
+// at rows + b rows_stride).  A block
 // none of whose rows lies in j0-1 .. j1 returns at once: with zero_outside = 0
 // its output rows stay unwritten (the rows a curl of those faces reads lie
 // inside), with zero_outside = 1 it writes them as zeros (the transform of the
@@ -152,8 +167,9 @@ struct Mult {
 template <class D, int NG, class In, class Out>
 __global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
     xpass_kernel(In in, Out out, PlanT<typename D::Real> pl, int nrows, const int *__restrict__ rows = nullptr,
-                 int zero_outside = 0) {
+                 int zero_outside = 0, int rows_stride = 0) {
     if (rows != nullptr) {  // uniform over the block: before any barrier
+        rows += (long long)rows_stride * blockIdx.y;
         const int r0 = 2 * NG * (int)blockIdx.x + 1, r1 = r0 + 2 * NG - 1;
         if (r1 < rows[2] - 1 || r0 > rows[3]) {
             if (zero_outside) {
@@ -525,19 +541,25 @@ struct NonlinArgs {
     T *rest;              // ng x L: dt (1.5 N1 - 0.5 N2) + rhsbc, or nullptr
     const StepDev *prm;
     Grid g;
+    // Ensembles of cases of one shape, stacked case-major (batch b = case L + level - 1):
+    // per-case Reynolds numbers (null: g.Re) and callback values (prm[case] when set)
+    const double *re_tab = nullptr;
+    int prm_per_case = 0;
 };
 
 template <class T>
-__device__ __forceinline__ double avg_qx(const NonlinArgs<T> &a, const T *q, int lev, int i, int j) {
+__device__ __forceinline__ double avg_qx(const NonlinArgs<T> &a, const StepDev *prm, const T *q, int lev, int i,
+                                         int j) {
     const Grid &g = a.g;
-    return ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + base_flux_x(g, a.prm, lev, i, j) +
-            base_flux_x(g, a.prm, lev, i, j - 1)) / 2;
+    return ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + base_flux_x(g, prm, lev, i, j) +
+            base_flux_x(g, prm, lev, i, j - 1)) / 2;
 }
 template <class T>
-__device__ __forceinline__ double avg_qy(const NonlinArgs<T> &a, const T *q, long long nu, int lev, int i, int j) {
+__device__ __forceinline__ double avg_qy(const NonlinArgs<T> &a, const StepDev *prm, const T *q, long long nu, int lev,
+                                         int i, int j) {
     const Grid &g = a.g;
-    return ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + base_flux_y(g, a.prm, lev, i, j) +
-            base_flux_y(g, a.prm, lev, i - 1, j)) / 2;
+    return ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + base_flux_y(g, prm, lev, i, j) +
+            base_flux_y(g, prm, lev, i - 1, j)) / 2;
 }
 
 // Tile of the nonlinear kernel: kNlTX x kNlTY circulation points per block of
@@ -555,7 +577,9 @@ template <class T>
 __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a) {
     const Grid &g = a.g;
     const int nx = g.nx, ny = g.ny;
-    const int b = blockIdx.z, lev = b + 1;
+    const int b = blockIdx.z, lev = b % g.L + 1, cs = b / g.L;
+    const StepDev *prm = a.prm + (a.prm_per_case ? cs : 0);
+    const double Re = a.re_tab ? a.re_tab[cs] : g.Re;
     const int I0 = blockIdx.x * kNlTX, J0 = blockIdx.y * kNlTY;  // outputs I0+1..I0+TX, J0+1..J0+TY
     const long long nq = (long long)(nx + 1) * ny + (long long)nx * (ny + 1), ng = (long long)(nx - 1) * (ny - 1);
     const long long nu = (long long)(nx + 1) * ny;
@@ -569,7 +593,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a
     constexpr int NT = kNlTX * kNlBY;
     const double hc = gridstep(g, lev);
     // base_flux! of a static grid is U hc on every face (fluid.jl:22-32)
-    const double sbx = a.prm->fs[0] * hc, sby = a.prm->fs[1] * hc;
+    const double sbx = prm->fs[0] * hc, sby = prm->fs[1] * hc;
     const bool moving = g.grid_moving;
 #pragma unroll
     for (int e = tid; e < (kNlTY + 2) * kNlTX; e += NT) {
@@ -578,7 +602,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a
         double v = 0.0;
         if (i <= nx && j <= ny + 1) {
             if (moving)
-                v = avg_qy(a, q, nu, lev, i, j);
+                v = avg_qy(a, prm, q, nu, lev, i, j);
             else
                 v = ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + sby + sby) / 2;
         }
@@ -591,7 +615,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a
         double v = 0.0;
         if (i <= nx + 1 && j <= ny) {
             if (moving)
-                v = avg_qx(a, q, lev, i, j);
+                v = avg_qx(a, prm, q, lev, i, j);
             else
                 v = ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + sbx + sbx) / 2;
         }
@@ -633,7 +657,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a
             // rest = dt b1 N1 + dt b2 N2 + rhsbc (fluid.jl:487-493), rhsbc = apply_bc!(0, get_bc(..); fac)
             double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * (double)a.n2[b * ng + GI(I, J)];
             if (lev < g.L && on_ring(g, I, J)) {
-                const double fac = 0.25 * g.dt / (g.Re * (hc * hc));
+                const double fac = 0.25 * g.dt / (Re * (hc * hc));
                 v = v + apply_bc_at(0.0, C, g, I, J, fac);
             }
             a.rest[b * ng + GI(I, J)] = (T)v;
@@ -737,6 +761,33 @@ static __global__ void __launch_bounds__(256) binv_gemv_kernel(const double *__r
     if (s == 0 && row < n) part[(long long)blockIdx.y * n + row] = ((red[0][r] + red[1][r]) + red[2][r]) + red[3][r];
 }
 
+// binv_gemv_kernel for the cases of a batched ensemble group (case = blockIdx.z,
+// grid sized for the largest case): x = Binv Ftmp of each case into its partials.
+static __global__ void __launch_bounds__(256) binv_gemv_multi_kernel(const CaseView *__restrict__ tab) {
+    __shared__ double red[4][64];
+    const CaseView &cv = tab[blockIdx.z];
+    const int n = 2 * cv.P.np;
+    const int nchunk = (n + 63) / 64;
+    if ((int)blockIdx.x >= nchunk || (int)blockIdx.y >= nchunk) return;  // uniform over the block
+    const double *__restrict__ A = cv.Binv;
+    const double *__restrict__ z = cv.Ftmp;
+    const int r = threadIdx.x % 64, s = threadIdx.x / 64;
+    const int row = blockIdx.x * 64 + r;
+    const int cbeg = blockIdx.y * 64;
+    double acc = 0.0;
+    if (row < n) {
+        if (cbeg + 64 <= n) {
+#pragma unroll
+            for (int c = cbeg + s; c < cbeg + 64; c += 4) acc += A[row + (long long)n * c] * __ldg(&z[c]);
+        } else {
+            for (int c = cbeg + s; c < n; c += 4) acc += A[row + (long long)n * c] * __ldg(&z[c]);
+        }
+    }
+    red[s][r] = acc;
+    __syncthreads();
+    if (s == 0 && row < n) cv.part[(long long)blockIdx.y * n + row] = ((red[0][r] + red[1][r]) + red[2][r]) + red[3][r];
+}
+
 // F~b = sum of the chunk partials; update_vars! fb = F~b h / dt (problem.jl:676-685);
 // total force sum over panels (problem.jl:853-856).  One block.
 static __global__ void binv_reduce_kernel(const double *__restrict__ part, int nchunk, int n, double *__restrict__ fbt,
@@ -778,6 +829,43 @@ static __global__ void binv_reduce_kernel(const double *__restrict__ part, int n
         }
         total[0] = ax;
         total[1] = ay;
+    }
+}
+
+// binv_reduce_kernel for the cases of a batched ensemble group: one block per case.
+static __global__ void binv_reduce_multi_kernel(const CaseView *__restrict__ tab, double h, double dt) {
+    __shared__ double sx[32], sy[32];
+    const CaseView &cv = tab[blockIdx.x];
+    const int n = 2 * cv.P.np, np = n / 2, nchunk = (n + 63) / 64;
+    double tx = 0.0, ty = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double v = 0.0;
+        for (int c = 0; c < nchunk; ++c) v += cv.part[(long long)c * n + k];
+        cv.Fbt[k] = v;
+        const double f = v * h / dt;
+        cv.fb[k] = f;
+        if (k < np)
+            tx += f;
+        else
+            ty += f;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        tx += __shfl_xor_sync(0xffffffffu, tx, o);
+        ty += __shfl_xor_sync(0xffffffffu, ty, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sx[threadIdx.x >> 5] = tx;
+        sy[threadIdx.x >> 5] = ty;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ax = 0.0, ay = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            ax += sx[k];
+            ay += sy[k];
+        }
+        cv.total[0] = ax;
+        cv.total[1] = ay;
     }
 }
 

@@ -1,10 +1,12 @@
 """Ensembles of independent cases stepped together on one GPU.
 
 The reference steps one case per solver.  A single small case (a few hundred
-cells a side, three levels) fills only a few percent of a B200, so an ensemble
-enqueues every case's step on that case's own stream before waiting for any
-(`ibpm_ensemble_advance`); the cases' step graphs then run side by side.  Each
-case's results are exactly those of stepping it alone.
+cells a side, three levels) fills only a few percent of a B200.  An ensemble
+(`ibpm_ensemble_advance`) therefore batches its static-body cases of one shape
+(precision, nx, ny, levels, grid step, time step): their fields are stacked and
+each line pass, nonlinear term, curl and coupling kernel runs once over all of
+them, one CUDA graph per group step; the rest step side by side on their own
+streams.  Each case's results are exactly those of stepping it alone.
 """
 from __future__ import annotations
 
@@ -28,6 +30,12 @@ class Ensemble:
         rc = self.lib.ibpm_ensemble_create(arr, len(self.solvers), C.byref(self._h))
         if rc != _abi.IBPM_OK:
             raise _abi.IbpmError(rc, "ibpm_ensemble_create failed")
+
+    def groups(self):
+        """(number of batched groups, number of cases they hold)."""
+        ng, nb = C.c_int32(), C.c_int32()
+        self.lib.ibpm_ensemble_groups(self._h, C.byref(ng), C.byref(nb))
+        return ng.value, nb.value
 
     def close(self):
         if self._h:

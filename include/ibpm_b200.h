@@ -149,16 +149,27 @@ int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force);
 
 /* Ensembles: independent cases (handles of any sizes, bodies and precisions)
  * stepped together.  No counterpart in the reference, which steps one case per
- * solver.  ibpm_ensemble_advance enqueues every case's step on that case's own
- * stream before waiting for any, so the cases' step graphs run side by side;
- * params[k * n + c] holds step k of case c.  Each case's results are those of
- * stepping it alone.  Static-body cases overlap fully; a moving-body case waits
- * for its region check every step.  The ensemble does not own the handles. */
+ * solver.  Static-body, static-grid cases of one precision with equal nx, ny,
+ * levels, grid step and time step form a batched group: their fields are
+ * stacked in one allocation, every line pass, nonlinear term, curl and
+ * coarsening runs as one launch over all cases of the group, and so does the
+ * coupling (E, B^-1, E^T), each case on its own panels; a group's whole step
+ * is one CUDA graph.  Other cases step on their own streams.  All of them are
+ * enqueued before any is waited for; params[k * n + c] holds step k of case c.
+ * Each case's results are the bits of stepping it alone.  While grouped, a
+ * case's handle reads and writes its slot of the group's fields (its own
+ * field buffers are freed); destroying the ensemble copies every case back
+ * into buffers of its own, so destroy the ensemble before its handles.  A
+ * handle may appear once.  The ensemble does not own the handles.  The
+ * environment variable IBPM_ENSEMBLE_BATCH=0 at creation disables grouping
+ * (every case on its own stream). */
 typedef struct ibpm_ensemble ibpm_ensemble;
 int ibpm_ensemble_create(ibpm_handle *const *cases, int32_t n, ibpm_ensemble **out);
 int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_params *params);
 void ibpm_ensemble_destroy(ibpm_ensemble *e);
 const char *ibpm_ensemble_last_error(const ibpm_ensemble *e);
+/* The number of batched groups and of the cases they hold (NULL skips). */
+int ibpm_ensemble_groups(const ibpm_ensemble *e, int32_t *ngroups, int32_t *nbatched);
 
 int ibpm_get_time(ibpm_handle *h, int64_t *index, double *t);
 int ibpm_get_info(ibpm_handle *h, ibpm_info *info);

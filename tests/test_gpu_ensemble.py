@@ -55,3 +55,67 @@ def test_multi_step_call_with_time_varying_freestream(ib):
     many.advance_many(12)
     assert np.array_equal(one.getstate().Gamma, many.getstate().Gamma)
     assert np.array_equal(one.total_force(), many.total_force())
+
+
+def _gusty_cases(ib, n, Res, h=0.04, nx=96, ny=64, L=3):
+    """n static cylinders/plates of one shape (a batched group) with different
+    Reynolds numbers, origins and bodies, in a time-varying freestream."""
+    def gust(t):
+        return (1.0 + 0.3 * math.sin(30.0 * t), 0.1 * math.cos(20.0 * t))
+
+    out = []
+    for k in range(n):
+        W, H = nx * h, ny * h
+        x0 = -0.4 * H - 0.02 * k
+        fluid = ib.Fluid(grid=ib.fluid_grid(h=h, xlims=(x0, x0 + W), ylims=(-0.5 * H, 0.5 * H), nlevel=L),
+                         Re=Res[k % len(Res)], freestream_vel=gust)
+        if k % 2 == 0:
+            panels = ib.Curves.partition(ib.Curves.Circle(r=0.3 + 0.05 * k, center=(0.0, 0.0)), 40 + 7 * k)
+        else:
+            a = math.radians(10.0 * k)
+            panels = ib.Curves.partition(ib.Curves.LineSegment((-0.5 * math.cos(a), 0.5 * math.sin(a)),
+                                                               (0.5 * math.cos(a), -0.5 * math.sin(a))), 25 + 3 * k)
+        out.append(ib.Problem(fluid=fluid, bodies=ib.Bodies(b=ib.StaticBody(panels)), scheme=ib.CNAB(dt=0.006)))
+    return out
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_batched_group_matches_cases_stepped_alone(ib, prec):
+    """18 cases of one shape form one batched group (18 >= 16 fields also takes
+    the wide Y-pass blocks) and two more of another width a second group.
+    Every case's state and forces equal stepping it alone, bit for bit,
+    across calls of several steps with a time-varying freestream; after the
+    ensemble is destroyed each case steps on alone from where it was."""
+    probs = _gusty_cases(ib, 18, (60.0, 100.0, 150.0)) + _gusty_cases(ib, 2, (80.0,), nx=64)
+    alone = [ib.GpuCnabSolver(ib.State(p), precision=prec) for p in probs]
+    for s in alone:
+        s.advance_many(7)
+    together = [ib.GpuCnabSolver(ib.State(p), precision=prec) for p in probs]
+    ens = ib.Ensemble(together)
+    assert ens.groups() == (2, 20)
+    ens.advance_(3)
+    ens.advance_(1)
+    ens.advance_(3)
+    for a, b in zip(alone, together):
+        sa, sb = a.getstate(), b.getstate()
+        assert sa.index == sb.index == 7
+        assert np.array_equal(sa.Gamma, sb.Gamma)
+        assert np.array_equal(sa.q, sb.q)
+        assert np.array_equal(sa.psi, sb.psi)
+        assert np.array_equal(sa.nonlin[0], sb.nonlin[0]) and np.array_equal(sa.nonlin[1], sb.nonlin[1])
+        assert np.array_equal(a.total_force(), b.total_force())
+    ens.close()
+    for a, b in zip(alone, together):
+        a.advance_many(2)
+        b.advance_many(2)
+        assert np.array_equal(a.getstate().Gamma, b.getstate().Gamma)
+        assert np.array_equal(a.total_force(), b.total_force())
+
+
+def test_grouping_can_be_disabled(ib, monkeypatch):
+    probs = _gusty_cases(ib, 3, (100.0,))
+    monkeypatch.setenv("IBPM_ENSEMBLE_BATCH", "0")
+    ens = ib.Ensemble([ib.GpuCnabSolver(ib.State(p)) for p in probs])
+    assert ens.groups() == (0, 0)
+    ens.advance_(2)
+    assert np.isfinite(ens.total_forces()).all()
