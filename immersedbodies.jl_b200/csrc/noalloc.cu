@@ -21,7 +21,7 @@
 //    only enter the graph, and later eager calls would read unwritten tables.
 //  * b and x may be the same buffer: the first pass reads b into scratch and
 //    only the last pass writes x, in stream order.
-//  * Errors are read from each launch's own return code (cudaLaunchKernel), so
+//  * Errors are read from each launch's own return code (cudaLaunchKernelEx), so
 //    an error left pending by an unrelated earlier launch is not reported as
 //    this call's failure.
 //  * Every call shares g_scratch, which keeps the last call's contents: calls
@@ -93,30 +93,38 @@ bool plan_ok(int M, PlanT<double> &pl) {
     return (M / 2 + kTPF - 1) / kTPF <= kMaxE;
 }
 
+// Launches return their own error code (cudaLaunchKernelEx, whose template
+// form checks the arguments against the kernel's parameters).
+inline cudaLaunchConfig_t launch_cfg(dim3 grid, dim3 block, size_t smem, cudaStream_t st) {
+    cudaLaunchConfig_t c{};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = smem;
+    c.stream = st;
+    c.attrs = nullptr;
+    c.numAttrs = 0;
+    return c;
+}
+
 template <class D, class In, class Out>
 cudaError_t xpass_na(const PlanT<double> &pl, In in, Out out, int nrows, cudaStream_t st) {
     constexpr int NG = 2;
-    const dim3 grid(((nrows + 1) / 2 + NG - 1) / NG, 1);
-    const int *rows = nullptr;
-    int zero_outside = 0;
-    void *args[] = {&in, &out, const_cast<PlanT<double> *>(&pl), &nrows, &rows, &zero_outside};
-    return cudaLaunchKernel((const void *)xpass_kernel<D, NG, In, Out>, grid, dim3(NG * D::TPF), args,
-                            pass_smem<D>(pl.M, NG, NG), st);
+    const cudaLaunchConfig_t c =
+        launch_cfg(dim3(((nrows + 1) / 2 + NG - 1) / NG, 1), dim3(NG * D::TPF), pass_smem<D>(pl.M, NG, NG), st);
+    return cudaLaunchKernelEx(&c, xpass_kernel<D, NG, In, Out>, in, out, pl, nrows, (const int *)nullptr, 0, 0);
 }
 
 template <class D>
 cudaError_t ypass_na(const PlanT<double> &pl, const double *in, double *out, int ncols, Mult m, cudaStream_t st) {
     constexpr int NG = 2;
-    const dim3 grid((ncols + 2 * NG - 1) / (2 * NG), 1);
-    long long bs = 0;
-    void *args[] = {&in, &out, &bs, &ncols, const_cast<PlanT<double> *>(&pl), &m};
-    return cudaLaunchKernel((const void *)ypass_kernel<D, NG>, grid, dim3(NG * D::TPF), args,
-                            pass_smem<D>(pl.M, NG, NG), st);
+    const cudaLaunchConfig_t c =
+        launch_cfg(dim3((ncols + 2 * NG - 1) / (2 * NG), 1), dim3(NG * D::TPF), pass_smem<D>(pl.M, NG, NG), st);
+    return cudaLaunchKernelEx(&c, ypass_kernel<D, NG>, in, out, 0LL, ncols, pl, m);
 }
 
 cudaError_t tables_na(double2 *tw, double *sn, double *cs, int M, cudaStream_t st) {
-    void *args[] = {&tw, &sn, &cs, &M};
-    return cudaLaunchKernel((const void *)noalloc_tables_kernel, dim3(8), dim3(128), args, 0, st);
+    const cudaLaunchConfig_t c = launch_cfg(dim3(8), dim3(128), 0, st);
+    return cudaLaunchKernelEx(&c, noalloc_tables_kernel, tw, sn, cs, M);
 }
 
 }  // namespace
