@@ -57,14 +57,12 @@ def step_bytes_model(nx: int, ny: int, L: int, npanel: int, s: float = 1.0) -> f
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# dominant kernel, from one ncu capture (not measured by this run):
-#   ncu --set full --clock-control none -k regex:ypass_kernel -s 210 -c 1 \
-#       python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-chosen --no-learned --no-ensemble
-# on one B200; cold-cache replay of one single-level Y pass of the 1024^2 x 5 step.
-NCU_TRAFFIC = {"ypass_kernel": 8454912.0}
-NCU_TRAFFIC_RUN = ("ncu --set full capture of one ypass_kernel launch (1023^2 FP64 level) of "
-                   "`python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-chosen --no-learned --no-ensemble`; "
-                   "a constant, not measured by this run")
+# dominant kernel classes, each from one ncu capture (constants, not measured by
+# this run); the command of each capture is in NCU_TRAFFIC_RUN.
+NCU_TRAFFIC = {"ypass": 8454912.0}
+NCU_TRAFFIC_RUN = {"ypass": "ncu --set full --clock-control none -k regex:ypass_kernel -s 210 -c 1 python bench.py "
+                            "--steps 1 --warmup 3 --no-cpu-baseline --no-chosen --no-learned --no-ensemble: one "
+                            "single-level launch (1023^2 FP64), cold-cache replay"}
 
 
 def read_peaks():
@@ -503,18 +501,28 @@ def main():
     solver.profile(False)
 
     peak, peak_kind = read_peaks()
-    n_y, ms_y, b_y = kern["ypass"]
-    dom = "ypass_kernel (one level: DST along y, multiply by scale/Λ, DST along y)"
-    achieved = (b_y / n_y) / ((ms_y / n_y) / 1000.0) / 1e9 if n_y else None
-    traffic = NCU_TRAFFIC.get("ypass_kernel")
+    # the dominant kernel: the class with the largest device time per step; its
+    # achieved bandwidth is the algorithmic bytes of all its launches over their time
+    names = {"ypass": "ypass_kernel (DST along y, multiply by scale/Λ, DST along y)",
+             "xpass": "xpass_kernel (DST along x of row pairs, with the solves' prologues and epilogues)",
+             "nonlinear": "nonlinear_kernel", "curl": "curl_kernel", "xtrial": "xpass_trial_kernel",
+             "ytrial": "ypass_trial_kernel"}
+    dom_key = max(kern, key=lambda k: kern[k][1])
+    n_d, ms_d, b_d = kern[dom_key]
+    achieved = b_d / (ms_d / 1000.0) / 1e9 if n_d else None
+    traffic = NCU_TRAFFIC.get(dom_key)
     step_bytes = step_bytes_model(nx, ny, L, prob.bodies.npanel)
-    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    n_y, ms_y, b_y = kern["ypass"]
+    roofline = {"kernel": names[dom_key], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": traffic,
-                "traffic_source": traffic and NCU_TRAFFIC_RUN,
+                "traffic_source": traffic and NCU_TRAFFIC_RUN.get(dom_key),
                 "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": b_y / n_y if n_y else None,
-                "launch_ms": ms_y / n_y if n_y else None,
+                "launches_per_step": n_d / prof_steps if n_d else None,
+                "algorithmic_bytes_per_launch": b_d / n_d if n_d else None,
+                "launch_ms": ms_d / n_d if n_d else None,
                 "kernel_ms_per_step": {k: v[1] / prof_steps for k, v in kern.items()},
+                "single_level_ypass": {"achieved": (b_y / n_y) / ((ms_y / n_y) / 1000.0) / 1e9 if n_y else None,
+                                       "launch_ms": ms_y / n_y if n_y else None},
                 "timing": f"CUDA events around each launch during {prof_steps} profiled steps (eager launches) "
                           "after the timed region",
                 "step": {"algorithmic_bytes": step_bytes, "achieved": step_bytes / (ms_step / 1000.0) / 1e9,

@@ -85,6 +85,7 @@ EXPORTS = {
     "ibpm_ensemble_destroy": (None, [C.c_void_p]),
     "ibpm_ensemble_last_error": (C.c_char_p, [C.c_void_p]),
     "ibpm_ensemble_groups": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "ibpm_tune_table": (C.c_int, [C.c_char_p, C.c_int32]),
     "ibpm_net_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
                                   C.POINTER(C.c_void_p)]),
     "ibpm_net_destroy": (None, [C.c_void_p]),
@@ -155,3 +156,17 @@ def fptr(a):
     if a.dtype != np.float32 or not a.flags.c_contiguous:
         raise ValueError("expected a C-contiguous float32 array")
     return a.ctypes.data_as(_fp)
+
+
+def tune_table() -> dict:
+    """The pass-shape autotuner's choices so far: {key: line pairs per block}."""
+    lib = load()
+    n = lib.ibpm_tune_table(None, 0)
+    buf = C.create_string_buffer(max(n, 1))
+    lib.ibpm_tune_table(buf, n)
+    out = {}
+    for line in buf.value.decode().splitlines():
+        k, _, v = line.rpartition(" ")
+        if k:
+            out[k] = int(v)
+    return out

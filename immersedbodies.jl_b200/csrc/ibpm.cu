@@ -20,8 +20,12 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <fstream>
 #include <initializer_list>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <sstream>
 #include <vector>
 
 #include "../../include/ibpm_b200.h"
@@ -101,6 +105,84 @@ bool make_plan(int M, PlanT<T> &pl) {
         if (K * R > kMaxV) return false;
     }
     return (M / 2 + kTPF - 1) / kTPF <= kMaxE;
+}
+
+// ---- pass-shape autotuner ----
+// The Y pass (DST along y, spectral multiply, DST along y) runs with NG line
+// pairs (2 NG columns) per block, NG in {1, 2, 4, 8}.  Every NG evaluates the
+// same per-line arithmetic, so the choice changes speed only, never results.
+// The best NG depends on the transform length, the precision and how many
+// fields one launch covers (one level, all levels, an ensemble group, a batch
+// of B columns), so the table is keyed by (GPU name, transform length,
+// precision, batch bucket).  With IBPM_TUNE=1 an engine times every NG on its
+// own scratch fields for each key it will launch (before any graph capture) and
+// keeps the fastest; IBPM_TUNE_CACHE names a text file the table is read from
+// at first use and appended to after tuning, so later processes start tuned.
+// Keys never tuned use the fixed rule (NG = 2, NG = 4 from 16 fields).
+// IBPM_TUNE_FORCE_NG forces one NG everywhere (a test knob).
+constexpr int kTuneNGs[4] = {1, 2, 4, 8};
+inline int batch_bucket(int nb) { return nb <= 1 ? 0 : nb <= 4 ? 1 : nb <= 15 ? 2 : nb <= 63 ? 3 : 4; }
+
+struct TuneTable {
+    std::mutex mu;
+    std::map<std::string, int> ng;  // key -> NG
+    bool loaded = false;
+    std::string path;
+    // (re)reads the cache file named by IBPM_TUNE_CACHE when that name changes;
+    // its entries replace the table's
+    void load_locked() {
+        const char *p = getenv("IBPM_TUNE_CACHE");
+        const std::string want = p ? p : "";
+        if (loaded && want == path) return;
+        loaded = true;
+        path = want;
+        if (path.empty()) return;
+        std::ifstream f(path);
+        std::string line;
+        while (std::getline(f, line)) {
+            const size_t at = line.rfind(' ');
+            if (at == std::string::npos) continue;
+            const int v = atoi(line.c_str() + at + 1);
+            if (v == 1 || v == 2 || v == 4 || v == 8) ng[line.substr(0, at)] = v;
+        }
+    }
+    bool find(const std::string &key, int *out) {
+        std::lock_guard<std::mutex> lk(mu);
+        load_locked();
+        auto it = ng.find(key);
+        if (it == ng.end()) return false;
+        *out = it->second;
+        return true;
+    }
+    void put(const std::string &key, int v) {
+        std::lock_guard<std::mutex> lk(mu);
+        load_locked();
+        ng[key] = v;
+        if (!path.empty()) {
+            std::ofstream f(path, std::ios::app);
+            f << key << ' ' << v << '\n';
+        }
+    }
+    std::string dump() {
+        std::lock_guard<std::mutex> lk(mu);
+        load_locked();
+        std::ostringstream o;
+        for (auto &kv : ng) o << kv.first << ' ' << kv.second << '\n';
+        return o.str();
+    }
+};
+TuneTable &tune_table() {
+    static TuneTable t;
+    return t;
+}
+bool tune_enabled() {
+    const char *e = getenv("IBPM_TUNE");
+    return e && e[0] == '1';
+}
+int tune_forced_ng() {
+    const char *e = getenv("IBPM_TUNE_FORCE_NG");
+    const int v = e ? atoi(e) : 0;
+    return (v == 1 || v == 2 || v == 4 || v == 8) ? v : 0;
 }
 
 }  // namespace
@@ -393,13 +475,82 @@ struct Engine final : ibpm_handle {
     template <class D>
     void ypass_t(const PlanT<typename D::Real> &pl, const typename D::Real *in, typename D::Real *out, long long bs,
                  int nbatch, Mult m) {
-        if constexpr (D::MC > 0) {
-            if (nbatch >= kWideBatch) {
-                ypass_launch<D, kNGWide>(pl, in, out, bs, nbatch, m);
-                return;
+        int ngy = ypass_ng<typename D::Real>(pl.M, nbatch, D::MC > 0);
+        ypass_ng_launch<D>(ngy, pl, in, out, bs, nbatch, m);
+    }
+    template <class D>
+    void ypass_ng_launch(int ngy, const PlanT<typename D::Real> &pl, const typename D::Real *in,
+                         typename D::Real *out, long long bs, int nbatch, Mult m) {
+        switch (ngy) {
+            case 1: ypass_launch<D, 1>(pl, in, out, bs, nbatch, m); break;
+            case 4: ypass_launch<D, 4>(pl, in, out, bs, nbatch, m); break;
+            case 8: ypass_launch<D, 8>(pl, in, out, bs, nbatch, m); break;
+            default: ypass_launch<D, 2>(pl, in, out, bs, nbatch, m); break;
+        }
+    }
+    // the autotuner's key of a Y pass of length M over nbatch fields
+    template <class R>
+    std::string ypass_key(int M, int nbatch) const {
+        cudaDeviceProp pr{};
+        cudaGetDeviceProperties(&pr, device);
+        return std::string(pr.name) + " ypass M=" + std::to_string(M) + (sizeof(R) == 8 ? " fp64" : " fp32") +
+               " batch=" + std::to_string(batch_bucket(nbatch));
+    }
+    // line pairs per block of a Y pass: forced, tuned, or the fixed rule
+    template <class R>
+    int ypass_ng(int M, int nbatch, bool compile_time) {
+        if (const int f = tune_forced_ng()) return f;
+        int v = 0;
+        if (tune_table().find(ypass_key<R>(M, nbatch), &v)) return v;
+        return compile_time && nbatch >= kWideBatch ? kNGWide : kNG;
+    }
+    // Times every NG of the Y pass over nbatch fields (scratch in -> out, at
+    // least nbatch * ng elements each) and records the fastest; eager only.
+    template <class R>
+    void tune_ypass(const R *in, R *out, int nbatch) {
+        if (!tune_enabled() || tune_forced_ng()) return;
+        const PlanT<R> &pl = plan_y<R>();
+        const std::string key = ypass_key<R>(pl.M, nbatch);
+        int have = 0;
+        if (tune_table().find(key, &have)) return;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CK(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return;
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        float best = 1e30f;
+        int best_ng = kNG;
+        for (int ngy : kTuneNGs) {
+            auto run = [&] {
+                switch (pl.M) {
+                    case 1024: ypass_ng_launch<Pow2Dst<1024, R>>(ngy, pl, in, out, ng, nbatch, mult(MULT_LAPINV, 1, 0)); break;
+                    case 512: ypass_ng_launch<Pow2Dst<512, R>>(ngy, pl, in, out, ng, nbatch, mult(MULT_LAPINV, 1, 0)); break;
+                    case 256: ypass_ng_launch<Pow2Dst<256, R>>(ngy, pl, in, out, ng, nbatch, mult(MULT_LAPINV, 1, 0)); break;
+                    case 384: ypass_ng_launch<MixDst<384, R>>(ngy, pl, in, out, ng, nbatch, mult(MULT_LAPINV, 1, 0)); break;
+                    default: ypass_ng_launch<GenericDst<R>>(ngy, pl, in, out, ng, nbatch, mult(MULT_LAPINV, 1, 0)); break;
+                }
+                CK(cudaGetLastError());
+            };
+            // a block of NG line pairs must fit the shared memory a block may use
+            const size_t need = (size_t)ngy * (size_t)(pl.M + 1 + (pl.M + 1) / 16 + 1) * 2 * sizeof(R) + 16 * 8 * ngy;
+            if (need > 220 * 1024) continue;
+            run();
+            run();
+            CK(cudaEventRecord(e0, st));
+            for (int k = 0; k < 5; ++k) run();
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                best_ng = ngy;
             }
         }
-        ypass_launch<D, kNG>(pl, in, out, bs, nbatch, m);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        tune_table().put(key, best_ng);
     }
     // Y pass with NGY line pairs (2 NGY columns) per block.  Launches over many
     // fields (the B assembly) have waves to spare, and wider blocks read longer
@@ -828,9 +979,13 @@ void Engine<T>::setup() {
     for (int b = 0; b < nbody; ++b)
         if (body_kind[b] == IBPM_BODY_STATIC) update_weights(body_start[b], body_start[b + 1]);
     check_region_error();
+    // pass shapes for one level and for all levels at once (scratch t1 -> t2)
+    tune_ypass<T>(t1, t2, 1);
+    if (L > 1) tune_ypass<T>(t1, t2, L);
     if (static_bodies) {
         compute_bbox();
         if (std::is_same<T, double>::value) {
+            if (kbatch > L) tune_ypass<T>(Gw, psiw, kbatch);
             build_Binv();
             shrink_batch_buffers();
         } else {
@@ -1912,6 +2067,8 @@ struct CaseGroup {
             CK(cudaMemcpyAsync(bbox_tab + 4 * c, ec.P.bbox, sizeof(int) * 4, cudaMemcpyDeviceToDevice, st));
         }
         CK(cudaMemcpyAsync(views, hv.data(), sizeof(CaseView) * C, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        e0->template tune_ypass<T>(t1, t2, C);  // the group's Y passes cover C fields
         // move every case's state into its slot and point the case there
         for (int c = 0; c < C; ++c) {
             Engine<T> &e = *cs[c];
@@ -2426,6 +2583,16 @@ int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_para
         return IBPM_WARN_CG_MAXITER;
     }
     return IBPM_OK;
+}
+
+int ibpm_tune_table(char *out, int32_t len) {
+    const std::string t = tune_table().dump();
+    if (out && len > 0) {
+        const size_t n = std::min<size_t>(t.size(), (size_t)len - 1);
+        memcpy(out, t.data(), n);
+        out[n] = 0;
+    }
+    return (int)t.size() + 1;
 }
 
 int ibpm_ensemble_groups(const ibpm_ensemble *e, int32_t *ngroups, int32_t *nbatched) {

@@ -171,6 +171,18 @@ const char *ibpm_ensemble_last_error(const ibpm_ensemble *e);
 /* The number of batched groups and of the cases they hold (NULL skips). */
 int ibpm_ensemble_groups(const ibpm_ensemble *e, int32_t *ngroups, int32_t *nbatched);
 
+/* Pass-shape autotuner (no counterpart in the reference).  The Y pass of the
+ * DST-diagonalised solves runs with NG line pairs (2 NG columns) per block, NG
+ * in {1, 2, 4, 8}; every NG gives the same bits.  With the environment variable
+ * IBPM_TUNE=1, engines (and ensemble groups) time every NG on the device for
+ * each (GPU, transform length, precision, batch bucket) they launch, before
+ * their first step, and keep the fastest; IBPM_TUNE_CACHE=<file> reads the table
+ * from that file at first use and appends new choices to it.  Untuned keys use
+ * NG = 2 (4 from 16 fields per launch).  IBPM_TUNE_FORCE_NG=<n> forces one NG.
+ * ibpm_tune_table writes the table as text lines "key NG" into out (len bytes,
+ * NUL-terminated) and returns the length it needs. */
+int ibpm_tune_table(char *out, int32_t len);
+
 int ibpm_get_time(ibpm_handle *h, int64_t *index, double *t);
 int ibpm_get_info(ibpm_handle *h, ibpm_info *info);
 const char *ibpm_last_error(const ibpm_handle *h);
