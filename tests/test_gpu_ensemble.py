@@ -57,26 +57,17 @@ def test_multi_step_call_with_time_varying_freestream(ib):
     assert np.array_equal(one.total_force(), many.total_force())
 
 
-def _gusty_cases(ib, n, Res, h=0.04, nx=96, ny=64, L=3):
-    """n static cylinders/plates of one shape (a batched group) with different
-    Reynolds numbers, origins and bodies, in a time-varying freestream."""
+def _gusty_cases(ib, n, seed, width):
+    """n seeded cylinders and plates of one shape (a batched group: width x 64
+    cells at h 0.04, 3 levels) with different Reynolds numbers and bodies, in a
+    time-varying freestream."""
     def gust(t):
         return (1.0 + 0.3 * math.sin(30.0 * t), 0.1 * math.cos(20.0 * t))
 
-    out = []
-    for k in range(n):
-        W, H = nx * h, ny * h
-        x0 = -0.4 * H - 0.02 * k
-        fluid = ib.Fluid(grid=ib.fluid_grid(h=h, xlims=(x0, x0 + W), ylims=(-0.5 * H, 0.5 * H), nlevel=L),
-                         Re=Res[k % len(Res)], freestream_vel=gust)
-        if k % 2 == 0:
-            panels = ib.Curves.partition(ib.Curves.Circle(r=0.3 + 0.05 * k, center=(0.0, 0.0)), 40 + 7 * k)
-        else:
-            a = math.radians(10.0 * k)
-            panels = ib.Curves.partition(ib.Curves.LineSegment((-0.5 * math.cos(a), 0.5 * math.sin(a)),
-                                                               (0.5 * math.cos(a), -0.5 * math.sin(a))), 25 + 3 * k)
-        out.append(ib.Problem(fluid=fluid, bodies=ib.Bodies(b=ib.StaticBody(panels)), scheme=ib.CNAB(dt=0.006)))
-    return out
+    probs = ib.configs.ensemble_cases(n, seed=seed, h=0.04, widths=(width,), ny=64)
+    for p in probs:
+        p.fluid.freestream_vel = gust
+    return probs
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
@@ -86,7 +77,7 @@ def test_batched_group_matches_cases_stepped_alone(ib, prec):
     Every case's state and forces equal stepping it alone, bit for bit,
     across calls of several steps with a time-varying freestream; after the
     ensemble is destroyed each case steps on alone from where it was."""
-    probs = _gusty_cases(ib, 18, (60.0, 100.0, 150.0)) + _gusty_cases(ib, 2, (80.0,), nx=64)
+    probs = _gusty_cases(ib, 18, 11, 96) + _gusty_cases(ib, 2, 5, 64)
     alone = [ib.GpuCnabSolver(ib.State(p), precision=prec) for p in probs]
     for s in alone:
         s.advance_many(7)
@@ -113,7 +104,7 @@ def test_batched_group_matches_cases_stepped_alone(ib, prec):
 
 
 def test_grouping_can_be_disabled(ib, monkeypatch):
-    probs = _gusty_cases(ib, 3, (100.0,))
+    probs = _gusty_cases(ib, 3, 13, 96)
     monkeypatch.setenv("IBPM_ENSEMBLE_BATCH", "0")
     ens = ib.Ensemble([ib.GpuCnabSolver(ib.State(p)) for p in probs])
     assert ens.groups() == (0, 0)
