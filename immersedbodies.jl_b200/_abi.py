@@ -22,6 +22,7 @@ IBPM_ERR_NOMEM = -4
 IBPM_ERR_NONFINITE = -5
 IBPM_FP64 = 0
 IBPM_FP32 = 1
+IBPM_MIXED_L1 = 2
 
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)

@@ -601,17 +601,24 @@ struct Engine final : ibpm_handle {
     // per-batch coefficients dt / (2 Re hc^2) come from ctab)
     template <class D>
     void trial_t(const T *Gold, const T *rest_, T *Gnew, int nb, const double *ctab) {
+        trial_core<D>(Gold, rest_, Gnew, nb, ctab, t1, t2, rhs, plx, ply);
+    }
+    // the merged trial solve on fields of the transform's element type R, with
+    // scratch t1_, t2_, rhs_ (nb fields each) and the plans of R
+    template <class D, class R = typename D::Real>
+    void trial_core(const R *Gold, const R *rest_, R *Gnew, int nb, const double *ctab, R *t1_, R *t2_, R *rhs_,
+                    const PlanT<R> &px, const PlanT<R> &py) {
         {
             const dim3 grid((ny - 1 + kNG - 1) / kNG, nb);
-            const size_t sm = pass_smem<D>(plx.M, kNG, kNG);
+            const size_t sm = pass_smem<D>(px.M, kNG, kNG);
             const int pe = prof_begin();
-            xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1, t2, ng, nx - 1, plx, ny - 1);
+            xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1_, t2_, ng, nx - 1, px, ny - 1);
             check_launch();
-            prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(T) * (double)ng * nb);
+            prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(R) * (double)ng * nb);
         }
         {
             const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nb);
-            const size_t sm = pass_smem<D>(ply.M, 2 * kNG, kNG);
+            const size_t sm = pass_smem<D>(py.M, 2 * kNG, kNG);
             // the cap must cover the largest M this instantiation serves (kMaxM); the
             // attribute is per device
             static std::atomic<unsigned long long> attr_devices{0};
@@ -623,11 +630,23 @@ struct Engine final : ibpm_handle {
             const int pe = prof_begin();
             Mult m = mult(MULT_AIMPL, 1, 1);
             m.coef_tab = ctab;
-            ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1, t2, rhs, ng, nx - 1, ply, m);
+            ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1_, t2_, rhs_, ng, nx - 1, py, m);
             check_launch();
-            prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(T) * (double)ng * nb);
+            prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(R) * (double)ng * nb);
         }
-        xpass(in_plain(rhs, ng), out_plain(Gnew, ng), nb);
+        xpass<R>(InPlain<R>{rhs_, ng, nx - 1}, OutPlain<R>{Gnew, ng, nx - 1}, nb);
+    }
+    // the merged trial solve of one FP64 level (IBPM_MIXED_L1's level 1)
+    void trial_d(const double *Gold, const double *rest_, double *Gnew) {
+        const PlanT<double> &px = plan_x<double>(), &py = plan_y<double>();
+        if (px.M == 1024 && py.M == 1024)
+            trial_core<Pow2Dst<1024, double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
+        else if (px.M == 512 && py.M == 512)
+            trial_core<Pow2Dst<512, double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
+        else if (px.M == 256 && py.M == 256)
+            trial_core<Pow2Dst<256, double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
+        else
+            trial_core<GenericDst<double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
     }
     void trial(const T *Gold, const T *rest_, T *Gnew, int nb = 0, const double *ctab = nullptr) {
         if (nb == 0) nb = L;
@@ -775,6 +794,14 @@ struct Engine final : ibpm_handle {
 
     void init(const ibpm_problem *p, const ibpm_options &o);
     bool hi_level1 = false;
+    // IBPM_MIXED_L1: level 1 (the body's level) kept and solved in FP64 (G1, q1,
+    // psi1, nl1 and FP64 scratch); the float arrays hold levels 2..L
+    bool l1d = false;
+    double *G1[2] = {nullptr, nullptr}, *nl1[2] = {nullptr, nullptr};
+    double *q1 = nullptr, *psi1 = nullptr, *rest1 = nullptr, *t1d = nullptr, *t2d = nullptr, *rhsd = nullptr;
+    double *patch_d = nullptr, *q0d = nullptr, *coef_coarse = nullptr;
+    void step_body_l1d();
+    void vort2flux_l1d(const double *G1v, T *Gm, T *qout, double *psi1_out, double *q1_out, bool curl_all);
     ibpm_problem problem_copy{};
     T *diag_q = nullptr, *diag_g = nullptr;  // diag_vort2flux buffers
     void set_state(const ibpm_state_view *s) override;
@@ -887,6 +914,31 @@ void Engine<T>::setup() {
         qs1_hi = dalloc<double>(nq);
         t1_hi = dalloc<double>(ng);
         t2_hi = dalloc<double>(ng);
+        l1d = opt.precision == IBPM_MIXED_L1;
+        if (l1d) {
+            if (!static_bodies)
+                throw ApiError{IBPM_ERR_INVALID, "the level-1-FP64 mixed precision needs static bodies"};
+            for (int k = 0; k < 2; ++k) {
+                G1[k] = dalloc<double>(ng);
+                nl1[k] = dalloc<double>(ng);
+            }
+            q1 = dalloc<double>(nq);
+            psi1 = dalloc<double>(ng);
+            rest1 = dalloc<double>(ng);
+            t1d = dalloc<double>(ng);
+            t2d = dalloc<double>(ng);
+            rhsd = dalloc<double>(ng);
+            q0d = dalloc<double>(nq);
+            patch_d = dalloc<double>(2LL * (nx + 1) * (ny + 1));
+            // dt / (2 Re hc^2) of levels 2..L, as Mult::coef forms it on the device
+            std::vector<double> cc(std::max(L - 1, 1), 0.0);
+            for (int lev = 2; lev <= L; ++lev) {
+                const double hc = ldexp(g.h, lev - 1);
+                cc[lev - 2] = g.dt / (2 * g.Re * (hc * hc));
+            }
+            coef_coarse = dalloc<double>(cc.size());
+            CK(cudaMemcpyAsync(coef_coarse, cc.data(), sizeof(double) * cc.size(), cudaMemcpyHostToDevice, st));
+        }
     }
 
     q = dalloc<T>(nq * L);
@@ -1405,6 +1457,10 @@ void Engine<T>::step(const ibpm_step_params &sp) {
 // The device work of one step after the per-step parameters are uploaded.
 template <class T>
 void Engine<T>::step_body() {
+    if (l1d) {
+        step_body_l1d();
+        return;
+    }
     const long long launches0 = launches;
     T *Gold = G[gc], *Gnew = G[1 - gc];
     T *N1 = nl[nc], *N2 = nl[1 - nc];
@@ -1521,6 +1577,101 @@ void Engine<T>::step_body() {
     vort2flux(psi, q, Gnew, 0, 0, 1, true);
     gc = 1 - gc;
     graph_launches[1 - gc] = launches - launches0;
+}
+
+// IBPM_MIXED_L1's step: the body's level (level 1) in FP64 -- its Gamma, flux,
+// streamfunction and nonlinear history stored and its solves run in FP64 -- and
+// the coarser levels in FP32.  Level 1 feeds E (src/coupling.jl:236-250), whose
+// errors B^-1 amplifies, while the coarser levels reach level 1 only through its
+// boundary values, a smooth field.  Same sequence as step_body.
+template <class T>
+void Engine<T>::step_body_l1d() {
+    const long long launches0 = launches;
+    T *Gold = G[gc], *Gnew = G[1 - gc];
+    T *N1 = nl[nc], *N2 = nl[1 - nc];
+    double *G1o = G1[gc], *G1n = G1[1 - gc], *N11 = nl1[nc], *N12 = nl1[1 - nc];
+    const dim3 blk(kNlTX, kNlBY);
+    // nonlinear + rhs assembly (src/fluid.jl:467-493): level 1 in FP64, its coarser
+    // level's Gamma in FP32; levels 2..L in FP32
+    {
+        NonlinArgs<double, T> a{q1, G1o, N11, N12, rest1, prm, g};
+        a.coarse = L > 1 ? Gold + ng : nullptr;
+        const dim3 grd((nx - 1 + kNlTX - 1) / kNlTX, (ny - 1 + kNlTY - 1) / kNlTY, 1);
+        nonlinear_kernel<double, T><<<grd, blk, 0, st>>>(a);
+        check_launch();
+    }
+    if (L > 1) {
+        NonlinArgs<T> a{q + nq, Gold + ng, N1 + ng, N2 + ng, rest + ng, prm, g};
+        a.lev0 = 2;
+        const dim3 grd((nx - 1 + kNlTX - 1) / kNlTX, (ny - 1 + kNlTY - 1) / kNlTY, L - 1);
+        nonlinear_kernel<T><<<grd, blk, 0, st>>>(a);
+        check_launch();
+    }
+    trial_d(G1o, rest1, G1n);
+    if (L > 1) trial(Gold + ng, rest + ng, Gnew + ng, L - 1, coef_coarse);
+    nc = 1 - nc;  // _cycle!(state.nonlin)
+    // couple_surface_rigid from the FP64 level-1 trial flux
+    vort2flux_l1d(G1n, Gnew, nullptr, psi1_hi, qs1_hi, false);
+    launch_regT(P, qs1_hi, 0, Ftmp, 0, 1, 1, prm, g, st);
+    check_launch();
+    const int n = 2 * np, nchunk = (n + 63) / 64;
+    binv_gemv_kernel<<<dim3(nchunk, nchunk), 256, 0, st>>>(Binv, Ftmp, part, n);
+    check_launch();
+    binv_reduce_kernel<<<1, 1024, 0, st>>>(part, nchunk, n, Fbt, fb, total, g.h, g.dt, 1);
+    check_launch();
+    last_cg_iters = 0;
+    // project_circ (src/coupling.jl:218-230) on the FP64 level 1
+    launch_reg_patch<double>(P, Fbt, 2 * np, patch_d, patch_stride, 1, g, st);
+    check_launch();
+    xpass<double>(InRegRot<double>{Patch<double>{patch_d, P.bbox, patch_stride}}, OutPlain<double>{t1d, ng, nx - 1}, 1,
+                  P.bbox, 1);
+    ypass<double>(t1d, t2d, ng, 1, mult(MULT_AIMPL, 1, 0));
+    xpass<double>(InPlain<double>{t2d, ng, nx - 1}, OutSub<double>{G1n, ng, nx - 1}, 1);
+    // vort2flux!(state.psi, state.q, state.Gamma)
+    vort2flux_l1d(G1n, Gnew, q, psi1, q1, true);
+    gc = 1 - gc;
+    graph_launches[1 - gc] = launches - launches0;
+}
+
+// vort2flux (src/fluid.jl:178-205) with level 1 in FP64 (G1v; psi1_out, q1_out)
+// and levels 2..L in FP32 (Gm, psi, qout; level slots as in the all-float layout,
+// slot 1 unused).  curl_all = false computes q at level 1 only.
+template <class T>
+void Engine<T>::vort2flux_l1d(const double *G1v, T *Gm, T *qout, double *psi1_out, double *q1_out, bool curl_all) {
+    const int nx2 = nx / 2, ny2 = ny / 2;
+    const dim3 cblk(16, 16), cgrd((nx2 + 15) / 16, (ny2 + 15) / 16, 1);
+    if (L >= 2) {
+        coarsify_kernel<T, double><<<cgrd, cblk, 0, st>>>(Gm + ng, G1v, 0, g);
+        check_launch();
+    }
+    for (int lev = 3; lev <= L; ++lev) {
+        coarsify_kernel<T><<<cgrd, cblk, 0, st>>>(Gm + (lev - 1) * ng, Gm + (lev - 2) * ng, 0, g);
+        check_launch();
+    }
+    const dim3 qblk(64, 4), qgrd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, 1);
+    for (int lev = L; lev >= 2; --lev) {
+        T *Gl = Gm + (lev - 1) * ng, *Pl = psi + (lev - 1) * ng;
+        if (lev == L)
+            xpass(in_plain(Gl, 0), out_plain(t1, ng), 1);
+        else
+            xpass(InBC<T>{Gl, psi + lev * ng, 0, 0, g}, out_plain(t1, ng), 1);
+        ypass(t1, t2, ng, 1, mult(MULT_LAPINV, 1, 0));
+        xpass(in_plain(t2, ng), out_plain(Pl, 0), 1);
+        if (curl_all) {
+            curl_kernel<T, T, T><<<qgrd, qblk, 0, st>>>(qout + (lev - 1) * nq, 0, Pl, 0,
+                                                        lev < L ? psi + lev * ng : nullptr, 0, g);
+            check_launch();
+        }
+    }
+    const T *coarse = L > 1 ? psi + ng : nullptr;
+    if (coarse)
+        xpass<double>(InBC<double, T>{G1v, coarse, 0, 0, g}, OutPlain<double>{t1d, ng, nx - 1}, 1);
+    else
+        xpass<double>(InPlain<double>{G1v, 0, nx - 1}, OutPlain<double>{t1d, ng, nx - 1}, 1);
+    ypass<double>(t1d, t2d, ng, 1, mult(MULT_LAPINV, 1, 0));
+    xpass<double>(InPlain<double>{t2d, ng, nx - 1}, OutPlain<double>{psi1_out, ng, nx - 1}, 1);
+    curl_kernel<double, double, T><<<qgrd, qblk, 0, st>>>(q1_out, 0, psi1_out, 0, coarse, 0, g);
+    check_launch();
 }
 
 namespace {
@@ -1665,7 +1816,17 @@ void Engine<T>::get_field(int field, int level, double *out) {
     if (!out) throw ApiError{IBPM_ERR_INVALID, "null output"};
     if (!field_d) field_d = dalloc<double>((size_t)std::max<long long>(nq, ng));
     if (field != IBPM_FIELD_VORTICITY) materialise_q0();
-    field_kernel<T><<<592, 256, 0, st>>>(G[gc], q, q0mat, field, level, g, field_d);
+    if (l1d && level == 1) {
+        // level 1 from its FP64 fields (q0 of the last step's callback values)
+        if (field != IBPM_FIELD_VORTICITY) {
+            q0_fill_kernel<double><<<dim3((unsigned)((nq + 255) / 256), 1), 256, 0, st>>>(q0d, prm, g);
+            check_launch();
+            if (q0_zero) CK(cudaMemsetAsync(q0d, 0, sizeof(double) * nq, st));
+        }
+        field_kernel<double><<<592, 256, 0, st>>>(G1[gc], q1, q0d, field, 1, g, field_d);
+    } else {
+        field_kernel<T><<<592, 256, 0, st>>>(G[gc], q, q0mat, field, level, g, field_d);
+    }
     check_launch();
     CK(cudaMemcpyAsync(out, field_d, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1767,6 +1928,14 @@ void Engine<T>::set_state(const ibpm_state_view *s) {
     if (s->psi) upload(psi, s->psi, ngL);
     if (s->nonlin1) upload(nl[nc], s->nonlin1, ngL);
     if (s->nonlin2) upload(nl[1 - nc], s->nonlin2, ngL);
+    if (l1d) {  // level 1 in FP64, exactly as given
+        const size_t bg = sizeof(double) * ng, bq = sizeof(double) * nq;
+        if (s->q) CK(cudaMemcpyAsync(q1, s->q, bq, cudaMemcpyHostToDevice, st));
+        if (s->gamma) CK(cudaMemcpyAsync(G1[gc], s->gamma, bg, cudaMemcpyHostToDevice, st));
+        if (s->psi) CK(cudaMemcpyAsync(psi1, s->psi, bg, cudaMemcpyHostToDevice, st));
+        if (s->nonlin1) CK(cudaMemcpyAsync(nl1[nc], s->nonlin1, bg, cudaMemcpyHostToDevice, st));
+        if (s->nonlin2) CK(cudaMemcpyAsync(nl1[1 - nc], s->nonlin2, bg, cudaMemcpyHostToDevice, st));
+    }
     if (s->xb) CK(cudaMemcpyAsync(P.xb, s->xb, np2, cudaMemcpyHostToDevice, st));
     if (s->ds) CK(cudaMemcpyAsync(ds, s->ds, np2 / 2, cudaMemcpyHostToDevice, st));
     if (s->ub) CK(cudaMemcpyAsync(P.ub, s->ub, np2, cudaMemcpyHostToDevice, st));
@@ -1802,6 +1971,20 @@ void Engine<T>::get_state(ibpm_state_view *s) {
     if (s->psi) download(s->psi, psi, ngL);
     if (s->nonlin1) download(s->nonlin1, nl[nc], ngL);
     if (s->nonlin2) download(s->nonlin2, nl[1 - nc], ngL);
+    if (l1d) {  // level 1 from its FP64 fields
+        const size_t bg = sizeof(double) * ng, bq = sizeof(double) * nq;
+        if (s->q) CK(cudaMemcpyAsync(s->q, q1, bq, cudaMemcpyDeviceToHost, st));
+        if (s->q0 && !q0_from_user) {  // prm holds the last step's values (materialise_q0 above)
+            q0_fill_kernel<double><<<dim3((unsigned)((nq + 255) / 256), 1), 256, 0, st>>>(q0d, prm, g);
+            check_launch();
+            if (q0_zero) CK(cudaMemsetAsync(q0d, 0, bq, st));
+            CK(cudaMemcpyAsync(s->q0, q0d, bq, cudaMemcpyDeviceToHost, st));
+        }
+        if (s->gamma) CK(cudaMemcpyAsync(s->gamma, G1[gc], bg, cudaMemcpyDeviceToHost, st));
+        if (s->psi) CK(cudaMemcpyAsync(s->psi, psi1, bg, cudaMemcpyDeviceToHost, st));
+        if (s->nonlin1) CK(cudaMemcpyAsync(s->nonlin1, nl1[nc], bg, cudaMemcpyDeviceToHost, st));
+        if (s->nonlin2) CK(cudaMemcpyAsync(s->nonlin2, nl1[1 - nc], bg, cudaMemcpyDeviceToHost, st));
+    }
     if (s->xb) CK(cudaMemcpyAsync(s->xb, P.xb, np2, cudaMemcpyDeviceToHost, st));
     if (s->ds) CK(cudaMemcpyAsync(s->ds, ds, np2 / 2, cudaMemcpyDeviceToHost, st));
     if (s->ub) CK(cudaMemcpyAsync(s->ub, P.ub, np2, cudaMemcpyDeviceToHost, st));
@@ -2003,7 +2186,7 @@ struct CaseGroup {
                e->g.dt == f->g.dt && e->hi_level1 == f->hi_level1;
     }
     static bool eligible(const Engine<T> *e) {
-        return e->static_bodies && !e->g.grid_moving && e->Binv != nullptr && !e->prof;
+        return e->static_bodies && !e->g.grid_moving && e->Binv != nullptr && !e->prof && !e->l1d;
     }
 
     void bind(const std::vector<Engine<T> *> &cases) {
@@ -2342,7 +2525,7 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
     ibpm_options opt;
     ibpm_default_options(&opt);
     if (opt_in) opt = *opt_in;
-    if (opt.precision != IBPM_FP64 && opt.precision != IBPM_FP32) {
+    if (opt.precision != IBPM_FP64 && opt.precision != IBPM_FP32 && opt.precision != IBPM_MIXED_L1) {
         g_create_error = "unsupported precision mode";
         return IBPM_ERR_INVALID;
     }
@@ -2399,7 +2582,7 @@ int ibpm_create(const ibpm_problem *p, const ibpm_options *opt_in, ibpm_handle *
         g_create_error = "no CUDA device available";
         return IBPM_ERR_CUDA;
     }
-    if (opt.precision == IBPM_FP32) return create_engine<float>(p, opt, out);
+    if (opt.precision == IBPM_FP32 || opt.precision == IBPM_MIXED_L1) return create_engine<float>(p, opt, out);
     return create_engine<double>(p, opt, out);
 }
 

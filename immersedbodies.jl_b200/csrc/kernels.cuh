@@ -37,10 +37,11 @@ struct InPlain {
 
 // Prologue of vort2flux's telescoping solve (src/fluid.jl:194-197):
 // Gamma_tmp = Gamma[:, lev]; apply_bc!(Gamma_tmp, get_bc(psi[:, lev+1]); fac=1)
-template <class T>
+// (the coarser level's psi may be of another element type TC)
+template <class T, class TC = T>
 struct InBC {
     const T *gam;
-    const T *coarse;
+    const TC *coarse;
     long long bs, cbs;
     Grid g;
     __device__ __forceinline__ double operator()(int b, int i, int j) const {
@@ -532,7 +533,7 @@ __global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
 
 // nonlinear (src/fluid.jl:441-455) = rot(direct_product(avg_flux(q + q0), Gamma, Gamma_bc)) / hc^2,
 // with Gamma_bc = 0.25 get_bc(Gamma[:, lev+1]) (src/fluid.jl:473-483).  Batch b = level - 1.
-template <class T>
+template <class T, class TC = T>
 struct NonlinArgs {
     const T *q;           // nq x L
     const T *gam;         // ng x L
@@ -545,18 +546,23 @@ struct NonlinArgs {
     // per-case Reynolds numbers (null: g.Re) and callback values (prm[case] when set)
     const double *re_tab = nullptr;
     int prm_per_case = 0;
+    // Fields that start at level lev0 (batch b is level lev0 + b % (L - lev0 + 1));
+    // coarse (element type TC), when set, is the Gamma of level lev0 + 1 (a field
+    // of another precision); otherwise a field's coarser level is the next batch.
+    int lev0 = 1;
+    const TC *coarse = nullptr;
 };
 
-template <class T>
-__device__ __forceinline__ double avg_qx(const NonlinArgs<T> &a, const StepDev *prm, const T *q, int lev, int i,
+template <class T, class TC>
+__device__ __forceinline__ double avg_qx(const NonlinArgs<T, TC> &a, const StepDev *prm, const T *q, int lev, int i,
                                          int j) {
     const Grid &g = a.g;
     return ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + base_flux_x(g, prm, lev, i, j) +
             base_flux_x(g, prm, lev, i, j - 1)) / 2;
 }
-template <class T>
-__device__ __forceinline__ double avg_qy(const NonlinArgs<T> &a, const StepDev *prm, const T *q, long long nu, int lev,
-                                         int i, int j) {
+template <class T, class TC>
+__device__ __forceinline__ double avg_qy(const NonlinArgs<T, TC> &a, const StepDev *prm, const T *q, long long nu,
+                                         int lev, int i, int j) {
     const Grid &g = a.g;
     return ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + base_flux_y(g, prm, lev, i, j) +
             base_flux_y(g, prm, lev, i - 1, j)) / 2;
@@ -573,11 +579,12 @@ constexpr int kNlTX = 32, kNlTY = 16, kNlBY = 8;
 // (direct_product_loops!) and the rot! difference are then formed from there, with
 // the reference's expressions, so each value rounds exactly as in a direct
 // evaluation.
-template <class T>
-__global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a) {
+template <class T, class TC = T>
+__global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T, TC> a) {
     const Grid &g = a.g;
     const int nx = g.nx, ny = g.ny;
-    const int b = blockIdx.z, lev = b % g.L + 1, cs = b / g.L;
+    const int nlev = g.L - a.lev0 + 1;
+    const int b = blockIdx.z, lev = a.lev0 + b % nlev, cs = b / nlev;
     const StepDev *prm = a.prm + (a.prm_per_case ? cs : 0);
     const double Re = a.re_tab ? a.re_tab[cs] : g.Re;
     const int I0 = blockIdx.x * kNlTX, J0 = blockIdx.y * kNlTY;  // outputs I0+1..I0+TX, J0+1..J0+TY
@@ -585,7 +592,13 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T> a
     const long long nu = (long long)(nx + 1) * ny;
     const T *q = a.q + b * nq;
     const T *Gt = a.gam + b * ng;
-    const T *C = lev < g.L ? a.gam + (b + 1) * ng : nullptr;
+    const TC *C = nullptr;
+    if (lev < g.L) {
+        if (a.coarse != nullptr)
+            C = a.coarse + cs * ng;
+        else if constexpr (std::is_same<T, TC>::value)
+            C = a.gam + (b + 1) * ng;
+    }
     __shared__ double aqy[kNlTY + 2][kNlTX];      // avg_qy(i, j), i = I0+2+x, j = J0+1+y
     __shared__ double aqx[kNlTY][kNlTX + 2];      // avg_qx(i, j), i = I0+1+x, j = J0+2+y
     __shared__ double gm[kNlTY + 2][kNlTX + 2];   // Gamma(i, j),  i = I0+x,   j = J0+y
@@ -720,16 +733,17 @@ __global__ void curl_kernel(T *__restrict__ qout, long long qbs, const TP *__res
     }
 }
 
-// coarsify! (src/fluid.jl:208-228): fine level -> central block of the next coarser level.
-template <class T>
-__global__ void coarsify_kernel(T *__restrict__ coarse, const T *__restrict__ fine, long long bs, Grid g) {
+// coarsify! (src/fluid.jl:208-228): fine level -> central block of the next coarser level
+// (the fine level may be of another element type TF).
+template <class T, class TF = T>
+__global__ void coarsify_kernel(T *__restrict__ coarse, const TF *__restrict__ fine, long long bs, Grid g) {
     const int nx = g.nx, ny = g.ny;
     const int ni = (nx / 2 - 2 - (-nx / 2 + 2)) / 2 + 1, nic = (nx / 4 - 1) - (-nx / 4 + 1) + 1;
     const int nj = (ny / 2 - 2 - (-ny / 2 + 2)) / 2 + 1, njc = (ny / 4 - 1) - (-ny / 4 + 1) + 1;
     const int ci = ni < nic ? ni : nic, cj = nj < njc ? nj : njc;
     const int a = blockIdx.x * blockDim.x + threadIdx.x, bb = blockIdx.y * blockDim.y + threadIdx.y;
     if (a >= ci || bb >= cj) return;
-    const T *Gf = fine + blockIdx.z * bs;
+    const TF *Gf = fine + blockIdx.z * bs;
     T *Gc = coarse + blockIdx.z * bs;
     auto G = [&](long long k) -> double { return (double)Gf[k]; };
     const int i = nx / 2 + (-nx / 2 + 2) + 2 * a, ic = nx / 2 + (-nx / 4 + 1) + a;

@@ -41,9 +41,10 @@ def _init_static_panels(state: State):
 class GpuCnabSolver(AbstractSolver):
     """CnabSolver(state; cg=(maxiter, reltol, abstol)) on the GPU.
 
-    precision="fp64" is the plain drop-in path; precision="fp32" is the mixed
-    precision path (FP32 fields and transforms; FP64 scans, boundary values,
-    CG, force sums and B^-1)."""
+    precision="fp64" is the plain drop-in path; precision="fp32" keeps every
+    level's fields and transforms in FP32 (FP64 scans, boundary values, CG,
+    force sums and B^-1); precision="mixed" keeps level 1, the body's level, in
+    FP64 and the coarser levels in FP32 (static bodies)."""
 
     def __init__(self, state: State, *, cg: Optional[dict] = None, device: int = 0, precision: str = "fp64"):
         self.lib = _abi.load()
@@ -65,7 +66,7 @@ class GpuCnabSolver(AbstractSolver):
         opt = _abi.ibpm_options()
         self.lib.ibpm_default_options(C.byref(opt))
         opt.device = device
-        opt.precision = {"fp64": _abi.IBPM_FP64, "fp32": _abi.IBPM_FP32}[precision]
+        opt.precision = {"fp64": _abi.IBPM_FP64, "fp32": _abi.IBPM_FP32, "mixed": _abi.IBPM_MIXED_L1}[precision]
         self.precision = precision
         for k, v in (cg or {}).items():
             setattr(opt, {"maxiter": "cg_maxiter", "reltol": "cg_reltol", "abstol": "cg_abstol"}[k], v)

@@ -59,6 +59,10 @@ extern "C" {
 #define IBPM_FP64 0                 /* plain FP64 drop-in path */
 #define IBPM_FP32 1                 /* mixed precision: FP32 fields and transforms; FP64 scans, boundary
                                        values, CG, force sums and B^-1 (no counterpart in the reference) */
+#define IBPM_MIXED_L1 2             /* mixed precision by level: level 1 (the body's level) stored and
+                                       solved in FP64, the coarser levels in FP32 fields and transforms;
+                                       FP64 scans, CG, force sums and B^-1; static bodies only (no
+                                       counterpart in the reference) */
 
 typedef struct ibpm_problem {
     int32_t nx, ny, nlevel;     /* MultiDomainGrid base.n and nlevel (problem.jl:398-409) */
@@ -75,7 +79,7 @@ typedef struct ibpm_problem {
 } ibpm_problem;
 
 typedef struct ibpm_options {
-    int32_t precision;          /* IBPM_FP64 or IBPM_FP32 */
+    int32_t precision;          /* IBPM_FP64, IBPM_FP32 or IBPM_MIXED_L1 */
     int32_t device;             /* CUDA device ordinal */
     int32_t cg_maxiter;         /* cg kwargs (solver.jl:137): maxiter, default 5000 */
     double cg_reltol;           /* default 1e-12 */

@@ -55,3 +55,47 @@ def test_fp32_moving_body_cg(ib):
         g64.advance_()
         g32.advance_()
     assert np.abs(g64.total_force() - g32.total_force()).max() <= TOL_COEF * max(1, np.abs(g64.total_force()).max())
+
+
+def _run_pair(ib, prob, nsteps, prec):
+    s64, sx = ib.State(prob), ib.State(prob)
+    g64 = ib.create_solver(s64, precision="fp64")
+    gx = ib.create_solver(sx, precision=prec)
+    worst = 0.0
+    for _ in range(nsteps):
+        g64.advance_()
+        gx.advance_()
+        worst = max(worst, float(np.abs(_coeffs(g64.total_force()) - _coeffs(gx.total_force())).max()))
+    g64.getstate()
+    gx.getstate()
+    return worst, rel_l2(sx.Gamma, s64.Gamma), s64, sx
+
+
+def test_mixed_level1_fp64_meets_the_bar_on_the_plate(ib):
+    """The chosen precision form (level 1 in FP64, levels 2..5 in FP32) on the
+    configured mixed-precision workload -- flat plate of chord 1 at 30 deg,
+    Re 200, 1024^2 x 5 levels, 201 points, dt 0.001, from rest -- over 200
+    steps against the FP64 path: |dC_D|, |dC_L| <= 1e-4 at every step and
+    vorticity relative L2 <= 1e-5 at the end (the bar of this form)."""
+    worst, vort, _, _ = _run_pair(ib, ib.configs.plate_aoa30_1024(), 200, "mixed")
+    assert worst <= 1e-4, worst
+    assert vort <= 1e-5, vort
+
+
+def test_mixed_level1_fp64_state_and_fields(ib):
+    """Level 1 of the mixed form is stored in FP64: a state set and read back
+    keeps its level-1 values exactly, and the level-1 vorticity accessor reads
+    the FP64 field."""
+    prob = ib.configs.small_cylinder(64, 3)
+    st = ib.configs.seed_vorticity(ib.State(prob))
+    g0 = st.Gamma.copy()
+    s = ib.create_solver(st, precision="mixed")
+    back = s.sync()
+    assert np.array_equal(back.Gamma[:, 0], g0[:, 0])
+    assert np.allclose(back.Gamma[:, 1:], g0[:, 1:], rtol=1e-6, atol=0)
+    for _ in range(3):
+        s.advance_()
+    s.getstate()
+    hc = prob.grid.gridstep(1)
+    vort1 = s.vorticity(1)
+    assert np.array_equal(vort1.ravel(order="F"), st.Gamma[:, 0] / (hc * hc))
