@@ -59,10 +59,13 @@ def step_bytes_model(nx: int, ny: int, L: int, npanel: int, s: float = 1.0) -> f
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # dominant kernel classes, each from one ncu capture (constants, not measured by
 # this run); the command of each capture is in NCU_TRAFFIC_RUN.
-NCU_TRAFFIC = {"ypass": 8454912.0}
+NCU_TRAFFIC = {"ypass": 8454912.0, "xpass": 8417792.0}
 NCU_TRAFFIC_RUN = {"ypass": "ncu --set full --clock-control none -k regex:ypass_kernel -s 210 -c 1 python bench.py "
                             "--steps 1 --warmup 3 --no-cpu-baseline --no-chosen --no-learned --no-ensemble: one "
-                            "single-level launch (1023^2 FP64), cold-cache replay"}
+                            "single-level launch (1023^2 FP64), cold-cache replay",
+                   "xpass": "ncu --set full --clock-control none --nvtx --nvtx-include timed/ -k regex:xpass_kernel "
+                            "-s 1 -c 1 python bench.py --steps 2 --warmup 3 --no-cpu-baseline --no-chosen --no-learned "
+                            "--no-ensemble: one single-level launch (1023^2 FP64, vort2flux level 5), cold-cache replay"}
 
 
 def read_peaks():

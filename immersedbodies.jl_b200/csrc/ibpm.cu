@@ -489,11 +489,10 @@ struct Engine final : ibpm_handle {
         }
     }
     // the autotuner's key of a Y pass of length M over nbatch fields
+    std::string devname;  // the GPU's name, read once at setup (a tuning key's first part)
     template <class R>
     std::string ypass_key(int M, int nbatch) const {
-        cudaDeviceProp pr{};
-        cudaGetDeviceProperties(&pr, device);
-        return std::string(pr.name) + " ypass M=" + std::to_string(M) + (sizeof(R) == 8 ? " fp64" : " fp32") +
+        return devname + " ypass M=" + std::to_string(M) + (sizeof(R) == 8 ? " fp64" : " fp32") +
                " batch=" + std::to_string(batch_bucket(nbatch));
     }
     // line pairs per block of a Y pass: forced, tuned, or the fixed rule
@@ -859,6 +858,11 @@ template <class T>
 void Engine<T>::setup() {
     CK(cudaSetDevice(device));
     if (const char *e = getenv("IBPM_NO_GRAPHS")) use_graphs = e[0] == '0';
+    {
+        cudaDeviceProp pr{};
+        CK(cudaGetDeviceProperties(&pr, device));
+        devname = pr.name;
+    }
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     if (!make_plan(nx, plx) || !make_plan(ny, ply))
         throw ApiError{IBPM_ERR_INVALID, "nx and ny must be even, <= 1024 and of the form 2^a 3^b 5^c"};
