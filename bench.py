@@ -406,8 +406,10 @@ def run_reference(args, world, rank):
         return
     ib = load_package()
     threads = os.cpu_count() or 1
-    steps = max(1, min(args.steps, 10))
-    warm = max(1, min(args.warmup, 2))
+    # the GPU arm's own steps and warm-up (a CPU step of the full case takes a
+    # fraction of a second on all host threads); capped so the run stays within minutes
+    steps = max(1, min(args.steps, 200))
+    warm = max(1, min(args.warmup, 20))
     v, used = cpu_time_oracle(ib, steps, warm, threads)
     line = {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
