@@ -1601,14 +1601,14 @@ void Engine<T>::step_body_l1d() {
         NonlinArgs<double, T> a{q1, G1o, N11, N12, rest1, prm, g};
         a.coarse = L > 1 ? Gold + ng : nullptr;
         const dim3 grd((nx - 1 + kNlTX - 1) / kNlTX, (ny - 1 + kNlTY - 1) / kNlTY, 1);
-        nonlinear_kernel<double, T><<<grd, blk, 0, st>>>(a);
+        nonlinear_kernel<double, T, true><<<grd, blk, 0, st>>>(a);
         check_launch();
     }
     if (L > 1) {
         NonlinArgs<T> a{q + nq, Gold + ng, N1 + ng, N2 + ng, rest + ng, prm, g};
         a.lev0 = 2;
         const dim3 grd((nx - 1 + kNlTX - 1) / kNlTX, (ny - 1 + kNlTY - 1) / kNlTY, L - 1);
-        nonlinear_kernel<T><<<grd, blk, 0, st>>>(a);
+        nonlinear_kernel<T, T, true><<<grd, blk, 0, st>>>(a);
         check_launch();
     }
     trial_d(G1o, rest1, G1n);
@@ -2380,7 +2380,7 @@ struct CaseGroup {
         {
             NonlinArgs<T> a{q, Gold, N1, N2, rest, prm_tab, e.g, re_tab, 1};
             const dim3 blk(kNlTX, kNlBY), grd((e.nx - 1 + kNlTX - 1) / kNlTX, (e.ny - 1 + kNlTY - 1) / kNlTY, C * L);
-            nonlinear_kernel<<<grd, blk, 0, st>>>(a);
+            nonlinear_kernel<T, T, true><<<grd, blk, 0, st>>>(a);
             e.check_launch();
         }
         e.trial(Gold, rest, Gnew, C * L, coef_all);

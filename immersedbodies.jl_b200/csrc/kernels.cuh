@@ -579,14 +579,23 @@ constexpr int kNlTX = 32, kNlTY = 16, kNlBY = 8;
 // (direct_product_loops!) and the rot! difference are then formed from there, with
 // the reference's expressions, so each value rounds exactly as in a direct
 // evaluation.
-template <class T, class TC = T>
-__global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T, TC> a) {
+// EXT: the ensemble / mixed-precision features of NonlinArgs (levels from lev0,
+// per-case tables, a coarse field of another type); without them the kernel
+// keeps the single-case code (fewer live registers, more resident blocks).
+template <class T, class TC = T, bool EXT = false>
+__global__ void __launch_bounds__(kNlTX *kNlBY, EXT ? 4 : 5) nonlinear_kernel(NonlinArgs<T, TC> a) {
     const Grid &g = a.g;
     const int nx = g.nx, ny = g.ny;
-    const int nlev = g.L - a.lev0 + 1;
-    const int b = blockIdx.z, lev = a.lev0 + b % nlev, cs = b / nlev;
-    const StepDev *prm = a.prm + (a.prm_per_case ? cs : 0);
-    const double Re = a.re_tab ? a.re_tab[cs] : g.Re;
+    const int b = blockIdx.z;
+    int lev = b + 1, cs = 0;
+    if constexpr (EXT) {
+        const int nlev = g.L - a.lev0 + 1;
+        lev = a.lev0 + b % nlev;
+        cs = b / nlev;
+    }
+    // per-case values, formed where they are used (no register held across the kernel)
+    auto prm_of = [&]() -> const StepDev * { return EXT ? a.prm + (a.prm_per_case ? cs : 0) : a.prm; };
+    auto re_of = [&]() -> double { return (EXT && a.re_tab) ? a.re_tab[cs] : g.Re; };
     const int I0 = blockIdx.x * kNlTX, J0 = blockIdx.y * kNlTY;  // outputs I0+1..I0+TX, J0+1..J0+TY
     const long long nq = (long long)(nx + 1) * ny + (long long)nx * (ny + 1), ng = (long long)(nx - 1) * (ny - 1);
     const long long nu = (long long)(nx + 1) * ny;
@@ -594,7 +603,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T, T
     const T *Gt = a.gam + b * ng;
     const TC *C = nullptr;
     if (lev < g.L) {
-        if (a.coarse != nullptr)
+        if (EXT && a.coarse != nullptr)
             C = a.coarse + cs * ng;
         else if constexpr (std::is_same<T, TC>::value)
             C = a.gam + (b + 1) * ng;
@@ -606,7 +615,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T, T
     constexpr int NT = kNlTX * kNlBY;
     const double hc = gridstep(g, lev);
     // base_flux! of a static grid is U hc on every face (fluid.jl:22-32)
-    const double sbx = prm->fs[0] * hc, sby = prm->fs[1] * hc;
+    const double sbx = prm_of()->fs[0] * hc, sby = prm_of()->fs[1] * hc;
     const bool moving = g.grid_moving;
 #pragma unroll
     for (int e = tid; e < (kNlTY + 2) * kNlTX; e += NT) {
@@ -615,7 +624,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T, T
         double v = 0.0;
         if (i <= nx && j <= ny + 1) {
             if (moving)
-                v = avg_qy(a, prm, q, nu, lev, i, j);
+                v = avg_qy(a, prm_of(), q, nu, lev, i, j);
             else
                 v = ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + sby + sby) / 2;
         }
@@ -628,7 +637,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T, T
         double v = 0.0;
         if (i <= nx + 1 && j <= ny) {
             if (moving)
-                v = avg_qx(a, prm, q, lev, i, j);
+                v = avg_qx(a, prm_of(), q, lev, i, j);
             else
                 v = ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + sbx + sbx) / 2;
         }
@@ -670,7 +679,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY) nonlinear_kernel(NonlinArgs<T, T
             // rest = dt b1 N1 + dt b2 N2 + rhsbc (fluid.jl:487-493), rhsbc = apply_bc!(0, get_bc(..); fac)
             double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * (double)a.n2[b * ng + GI(I, J)];
             if (lev < g.L && on_ring(g, I, J)) {
-                const double fac = 0.25 * g.dt / (Re * (hc * hc));
+                const double fac = 0.25 * g.dt / (re_of() * (hc * hc));
                 v = v + apply_bc_at(0.0, C, g, I, J, fac);
             }
             a.rest[b * ng + GI(I, J)] = (T)v;
