@@ -212,7 +212,9 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
     out, forces = {}, {}
     runs = (("previous", "previous", 16), ("extrapolated", "extrapolated", 16), ("learned", "learned", 16),
             ("projected", "projected", 16), ("direct", "direct", 1), ("direct_every_8", "direct", 8),
-            ("preconditioned_every_8", "preconditioned", 8), ("preconditioned_every_32", "preconditioned", 32))
+            ("preconditioned_every_8", "preconditioned", 8), ("preconditioned_every_32", "preconditioned", 32),
+            ("preconditioned_extrapolated_every_8", "preconditioned_extrapolated", 8),
+            ("preconditioned_extrapolated_every_32", "preconditioned_extrapolated", 32))
     for label, mode, depth in runs:
         s = make(0.55)
         if mode != "previous":

@@ -106,7 +106,7 @@ EXPORTS = {
     "ibpm_noalloc_last_error": (C.c_char_p, []),
 }
 (IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED, IBPM_WS_PROJECTED, IBPM_WS_DIRECT,
- IBPM_WS_PRECONDITIONED) = 0, 1, 2, 3, 4, 5
+ IBPM_WS_PRECONDITIONED, IBPM_WS_PRECOND_EXTRAP) = 0, 1, 2, 3, 4, 5, 6
 KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5}
 
 _lib = None

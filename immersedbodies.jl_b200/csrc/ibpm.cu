@@ -277,7 +277,15 @@ struct Engine final : ibpm_handle {
     // IBPM_WS_DIRECT / IBPM_WS_PRECONDITIONED: B^-1 of the body position, rebuilt
     // every ws_refresh steps (ws_since counts the steps since the last rebuild) by
     // its own graph
-    bool uses_binv_start() const { return ws_mode == IBPM_WS_DIRECT || ws_mode == IBPM_WS_PRECONDITIONED; }
+    bool uses_binv_start() const {
+        return ws_mode == IBPM_WS_DIRECT || ws_mode == IBPM_WS_PRECONDITIONED || ws_mode == IBPM_WS_PRECOND_EXTRAP;
+    }
+    bool preconditioned() const { return ws_mode == IBPM_WS_PRECONDITIONED || ws_mode == IBPM_WS_PRECOND_EXTRAP; }
+    // IBPM_WS_PRECOND_EXTRAP: the last three stale errors e_k = F_k - Binv b_k (ring
+    // of 3 x 2np), this step's Binv b, and how many errors are valid since the
+    // last rebuild (device int)
+    double *ws_stale = nullptr, *ws_x0 = nullptr;
+    int *ws_nvalid = nullptr;
     int ws_refresh = 1;
     long long ws_since = 0;
     cudaGraph_t binv_graph = nullptr;
@@ -1196,6 +1204,39 @@ __global__ void cg_init_kernel(CgArgs a, cudaGraphConditionalHandle h, int use_h
     }
 }
 
+// IBPM_WS_PRECOND_EXTRAP's start: x0 = Binv b (in x) is kept, and x gets the
+// stale error e = F - Binv b of this step extrapolated from the last ones,
+// polynomially in time: e1, 2 e1 - e2 or 3 e1 - 3 e2 + e3 as 1, 2 or 3 are valid
+// (none right after a rebuild).  stale = [e1 | e2 | e3].
+__global__ void stale_start_kernel(double *__restrict__ x, double *__restrict__ x0,
+                                   const double *__restrict__ stale, int n, const int *__restrict__ nvalid) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int v = *nvalid;
+    const double b0 = x[k];
+    x0[k] = b0;
+    const double e1 = stale[k], e2 = stale[n + k], e3 = stale[2 * n + k];
+    double e = 0.0;
+    if (v >= 3)
+        e = 3.0 * e1 - 3.0 * e2 + e3;
+    else if (v == 2)
+        e = 2.0 * e1 - e2;
+    else if (v == 1)
+        e = e1;
+    x[k] = b0 + e;
+}
+// after CG: e_new = F - x0 enters the ring (e3 <- e2 <- e1 <- e_new), one block
+__global__ void stale_update_kernel(const double *__restrict__ f, const double *__restrict__ x0,
+                                    double *__restrict__ stale, int n, int *__restrict__ nvalid) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        stale[2 * n + k] = stale[n + k];
+        stale[n + k] = stale[k];
+        stale[k] = f[k] - x0[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *nvalid = min(*nvalid + 1, 3);
+}
+
 // ||b - c|| into *out (one block, the reduction of cg_init_kernel)
 __global__ void residual_norm_kernel(const double *__restrict__ b, const double *__restrict__ c, int n,
                                      double *__restrict__ out) {
@@ -1413,7 +1454,11 @@ void Engine<T>::step(const ibpm_step_params &sp) {
         compute_bbox();
         check_region_error();
         if (uses_binv_start()) {
-            if (ws_since % ws_refresh == 0) direct_rebuild();
+            if (ws_since % ws_refresh == 0) {
+                direct_rebuild();
+                // stale errors refer to the previous inverse
+                if (ws_nvalid) CK(cudaMemsetAsync(ws_nvalid, 0, sizeof(int), st));
+            }
             ++ws_since;
         }
     }
@@ -1527,7 +1572,15 @@ void Engine<T>::step_body() {
             check_launch();
             binv_reduce_kernel<<<1, 1024, 0, st>>>(part, nchunk, n, Fbt, fb, total, g.h, g.dt, 1);
             check_launch();
-            cg(Fbt, Ftmp, false, ws_mode == IBPM_WS_PRECONDITIONED, rref);
+            if (ws_mode == IBPM_WS_PRECOND_EXTRAP) {
+                stale_start_kernel<<<(n + 255) / 256, 256, 0, st>>>(Fbt, ws_x0, ws_stale, n, ws_nvalid);
+                check_launch();
+            }
+            cg(Fbt, Ftmp, false, preconditioned(), rref);
+            if (ws_mode == IBPM_WS_PRECOND_EXTRAP) {
+                stale_update_kernel<<<1, 256, 0, st>>>(Fbt, ws_x0, ws_stale, n, ws_nvalid);
+                check_launch();
+            }
         } else if (ws_mode == IBPM_WS_PROJECTED) {
             // Galerkin over the last ws_depth solutions, B applied to all in one batch
             apply_B(ws_hist, ws_bhist, 2 * np, ws_depth);
@@ -1841,9 +1894,15 @@ void Engine<T>::set_warm_start(ibpm_net *net, int mode, int depth) {
     CK(cudaSetDevice(device));
     if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
     if (mode != IBPM_WS_PREVIOUS && mode != IBPM_WS_LEARNED && mode != IBPM_WS_EXTRAPOLATED &&
-        mode != IBPM_WS_PROJECTED && mode != IBPM_WS_DIRECT && mode != IBPM_WS_PRECONDITIONED)
+        mode != IBPM_WS_PROJECTED && mode != IBPM_WS_DIRECT && mode != IBPM_WS_PRECONDITIONED &&
+        mode != IBPM_WS_PRECOND_EXTRAP)
         throw ApiError{IBPM_ERR_INVALID, "unknown warm-start mode"};
-    if (mode == IBPM_WS_DIRECT || mode == IBPM_WS_PRECONDITIONED) {
+    if (mode == IBPM_WS_PRECOND_EXTRAP && !ws_stale) {
+        ws_stale = dalloc<double>(6 * (size_t)np);
+        ws_x0 = dalloc<double>(2 * (size_t)np);
+        ws_nvalid = dalloc<int>(1);
+    }
+    if (mode == IBPM_WS_DIRECT || mode == IBPM_WS_PRECONDITIONED || mode == IBPM_WS_PRECOND_EXTRAP) {
         if (!std::is_same<T, double>::value)
             throw ApiError{IBPM_ERR_INVALID, "the direct and preconditioned starts need the FP64 engine"};
         if (depth < 1 || depth > (1 << 20)) throw ApiError{IBPM_ERR_INVALID, "the rebuild interval (depth) must be 1 .. 1048576"};

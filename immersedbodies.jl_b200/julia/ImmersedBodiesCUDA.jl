@@ -215,7 +215,8 @@ level_y_velocity(solver::GpuCnabSolver, level::Integer=1) =
 # preconditioned by that inverse (not the reference's iteration; same stopping
 # rule).  (The learned mode needs a network made with ibpm_net_*.)
 function set_warm_start!(solver::GpuCnabSolver, mode::Symbol=:projected; depth::Integer=16)
-    m = Dict(:previous => 0, :extrapolated => 2, :projected => 3, :direct => 4, :preconditioned => 5)[mode]
+    m = Dict(:previous => 0, :extrapolated => 2, :projected => 3, :direct => 4, :preconditioned => 5,
+        :preconditioned_extrapolated => 6)[mode]
     _check(solver.handle, ccall((:ibpm_set_warm_start, libibpm), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32),
         solver.handle, m, C_NULL, depth))
     solver

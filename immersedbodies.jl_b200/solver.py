@@ -241,12 +241,15 @@ class GpuCnabSolver(AbstractSolver):
         solutions), "direct" (B^-1 b, B assembled and inverted on the GPU every
         `depth` steps; FP64 only) or "preconditioned" (as "direct", and CG
         preconditioned by that inverse: a few iterations between rebuilds; not the
-        reference's unpreconditioned iteration).  Keep the network alive while it
-        is installed."""
+        reference's unpreconditioned iteration) or "preconditioned_extrapolated"
+        (as "preconditioned", started from B^-1 b plus the stale error
+        F - B^-1 b extrapolated from the last steps).  Keep the network alive
+        while it is installed."""
         mode = mode or ("learned" if net is not None else "previous")
         m = {"previous": _abi.IBPM_WS_PREVIOUS, "learned": _abi.IBPM_WS_LEARNED,
              "extrapolated": _abi.IBPM_WS_EXTRAPOLATED, "projected": _abi.IBPM_WS_PROJECTED,
-             "direct": _abi.IBPM_WS_DIRECT, "preconditioned": _abi.IBPM_WS_PRECONDITIONED}[mode]
+             "direct": _abi.IBPM_WS_DIRECT, "preconditioned": _abi.IBPM_WS_PRECONDITIONED,
+             "preconditioned_extrapolated": _abi.IBPM_WS_PRECOND_EXTRAP}[mode]
         _abi.check(self.lib, self._h, self.lib.ibpm_set_warm_start(self._h, m, net.handle if net is not None else None,
                                                                     depth))
         self._warm_net = net

@@ -308,6 +308,10 @@ const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed
 #define IBPM_WS_PROJECTED 3
 #define IBPM_WS_DIRECT 4
 #define IBPM_WS_PRECONDITIONED 5
+/* IBPM_WS_PRECONDITIONED with a better start between rebuilds: B^-1 b plus this
+ * step's stale error F - B^-1 b extrapolated in time from the last (up to
+ * three) steps' stale errors, which change smoothly with the body's motion. */
+#define IBPM_WS_PRECOND_EXTRAP 6
 int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t depth);
 /* The last step's warm-start features (10 x npanel floats), target (2 x
  * npanel: the converged F~b minus the extrapolated guess x_e) and, in the

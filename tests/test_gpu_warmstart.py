@@ -140,12 +140,31 @@ def test_preconditioned_cg_with_a_periodic_inverse(ib):
     assert it.max() <= 12 and it.mean() <= 0.1 * it0.mean(), (it, it0.mean())
 
 
+def test_preconditioned_extrapolated_start_saves_iterations(ib):
+    """The preconditioned mode started from B^-1 b plus the stale error F - B^-1 b
+    extrapolated from the last steps' (rebuild every 16th step): fewer CG
+    iterations between rebuilds than from B^-1 b alone, the same at rebuild
+    steps, and the reference start's forces to the CG tolerance."""
+    runs = {}
+    for mode in ("previous", "preconditioned", "preconditioned_extrapolated"):
+        s = _plate(ib, 0.5)
+        if mode != "previous":
+            s.set_warm_start(None, mode=mode, depth=16)
+        runs[mode] = (_iters(s, 48), s.total_force().copy())
+        del s
+    (_, f0), (itp, _), (ite, fe) = runs["previous"], runs["preconditioned"], runs["preconditioned_extrapolated"]
+    assert np.abs(fe - f0).max() <= 1e-6 * np.abs(f0).max()
+    assert ite[::16].max() <= 1
+    between = [k for k in range(len(ite)) if k % 16 >= 3]  # three stale errors known
+    assert ite[between].mean() < itp[between].mean() - 0.5, (ite, itp)
+
+
 def test_direct_and_preconditioned_eager_match_graphs(ib):
     """With kernel profiling on, steps run eagerly: the B^-1 rebuild without its
     graph and CG as a host loop.  Both modes give the graph path's iteration
     counts and forces."""
     out = {}
-    for mode in ("direct", "preconditioned"):
+    for mode in ("direct", "preconditioned", "preconditioned_extrapolated"):
         for eager in (False, True):
             s = _plate(ib, 0.5)
             s.set_warm_start(None, mode=mode, depth=4)
@@ -153,7 +172,7 @@ def test_direct_and_preconditioned_eager_match_graphs(ib):
                 s.profile(True)
             out[(mode, eager)] = (_iters(s, 10), s.total_force().copy())
             del s
-    for mode in ("direct", "preconditioned"):
+    for mode in ("direct", "preconditioned", "preconditioned_extrapolated"):
         (ig, fg), (ie, fe) = out[(mode, False)], out[(mode, True)]
         assert np.array_equal(ig, ie), (mode, ig, ie)
         assert np.abs(fe - fg).max() <= 1e-13 * np.abs(fg).max(), mode
