@@ -101,13 +101,14 @@ EXPORTS = {
                                  C.c_uint64, _fp]),
     "ibpm_net_last_error": (C.c_char_p, [C.c_void_p]),
     "ibpm_set_warm_start": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
+    "ibpm_set_rebuild_transform": (C.c_int, [C.c_void_p, C.c_int32]),
     "ibpm_warm_start_sample": (C.c_int, [C.c_void_p, _fp, _fp, _fp]),
     "ibpm_lap_inv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ibpm_noalloc_last_error": (C.c_char_p, []),
 }
 (IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED, IBPM_WS_PROJECTED, IBPM_WS_DIRECT,
  IBPM_WS_PRECONDITIONED, IBPM_WS_PRECOND_EXTRAP) = 0, 1, 2, 3, 4, 5, 6
-KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5}
+KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5, "tcdst": 6}
 
 _lib = None
 

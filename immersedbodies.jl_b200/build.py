@@ -3,8 +3,9 @@
 Translation units: ibpm.cu (transforms, stencils, host runtime and C ABI);
 coupling.cu, compiled with -fmad=false so the regularised-delta weights and the
 E / E^T sums round exactly like the reference (no fused multiply-add);
-noalloc.cu (the allocation-free Laplacian-inverse entry point); and
-warmstart.cu (the learned CG warm start's network).
+noalloc.cu (the allocation-free Laplacian-inverse entry point);
+warmstart.cu (the learned CG warm start's network); and tc_dst.cu (dense DST-I
+passes on the tensor cores for the preconditioner's B assembly).
 """
 from __future__ import annotations
 
@@ -19,7 +20,7 @@ OUT = os.path.join(HERE, "lib", "libibpm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "550"]
-UNITS = [("ibpm.cu", []), ("coupling.cu", ["-fmad=false"]), ("noalloc.cu", []), ("warmstart.cu", [])]
+UNITS = [("ibpm.cu", []), ("coupling.cu", ["-fmad=false"]), ("noalloc.cu", []), ("warmstart.cu", []), ("tc_dst.cu", [])]
 
 
 def _deps():

@@ -32,12 +32,21 @@
 #include "coupling.h"
 #include "warmstart.h"
 #include "kernels.cuh"
+#include "tc_dst.h"
 
 using namespace ibpm;
 
 namespace {
 
 constexpr int kNG = 2;  // FFT groups (line pairs) per block
+
+// Spectral multipliers of one level for the tensor-core transforms, as FP32
+// [ky][kx] (P x P, zero in the padding row and column)
+__global__ void tc_mult_kernel(Mult m, int P, float *tab) {
+    const int kx = blockIdx.x * blockDim.x + threadIdx.x, ky = blockIdx.y;
+    if (kx >= P) return;
+    tab[(size_t)ky * P + kx] = (kx < P - 1 && ky < P - 1) ? (float)m(m.coef(0), kx + 1, ky + 1) : 0.0f;
+}
 constexpr int kNGWide = 4, kWideBatch = 16;  // Y-pass groups per block for launches over >= kWideBatch fields
 
 thread_local std::string g_create_error;
@@ -212,6 +221,7 @@ struct ibpm_handle {
     virtual void diag_vort2flux(double *gamma, double *psi, double *q) = 0;
     virtual void diag_reg(const double *f, double *gamma1, const double *q1, double *fout) = 0;
     virtual void set_warm_start(ibpm_net *net, int mode, int depth) = 0;
+    virtual void set_rebuild_transform(int products) = 0;
     virtual void warm_start_sample(float *features, float *target, float *prediction) = 0;
 };
 
@@ -286,6 +296,15 @@ struct Engine final : ibpm_handle {
     // last rebuild (device int)
     double *ws_stale = nullptr, *ws_x0 = nullptr;
     int *ws_nvalid = nullptr;
+    // The preconditioned modes' B assembly on the tensor cores: tc_prod BF16
+    // products per transform (0: the FP64 transforms); tc_on while an assembly
+    // runs its solves there; multipliers [ky][kx] of level 1: Laplacian inverse
+    // and implicit diffusion (tc_mult[0], tc_mult[1]), any mode and level for
+    // ibpm_diag_solve (tc_mult[2])
+    int tc_prod = 0;
+    bool tc_on = false;
+    TcDstPlan *tc = nullptr;
+    float *tc_mult[3] = {nullptr, nullptr, nullptr};
     int ws_refresh = 1;
     long long ws_since = 0;
     cudaGraph_t binv_graph = nullptr;
@@ -426,6 +445,7 @@ struct Engine final : ibpm_handle {
     ~Engine() override {
         if (st) cudaStreamSynchronize(st);
         drop_graphs();
+        if (tc) tc_destroy(tc);
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         for (void *p : allocs) cudaFree(p);
         for (int k = 0; k < kStage; ++k) {
@@ -684,6 +704,49 @@ struct Engine final : ibpm_handle {
     InPlain<T> in_plain(const T *p, long long bs) const { return InPlain<T>{p, bs, nx - 1}; }
     OutPlain<T> out_plain(T *p, long long bs) const { return OutPlain<T>{p, bs, nx - 1}; }
 
+    // The tensor-core transforms for nf fields of nprod products: creates (or
+    // re-creates) the plan and the level-1 multiplier tables outside any capture.
+    // A new plan has new buffers, so the captured B rebuild is dropped.
+    void tc_prepare(int nf, int nprod) {
+        if (tc && tc_nprod(tc) == nprod && tc_fmax(tc) >= nf) return;
+        CK(cudaStreamSynchronize(st));
+        if (tc) {
+            tc_destroy(tc);
+            tc = nullptr;
+        }
+        if (binv_exec) cudaGraphExecDestroy(binv_exec);
+        if (binv_graph) cudaGraphDestroy(binv_graph);
+        binv_exec = nullptr;
+        binv_graph = nullptr;
+        const char *why = "tensor-core transforms unavailable";
+        tc = tc_create(nx, nf, nprod, &why);
+        if (!tc) {
+            (void)cudaGetLastError();
+            throw ApiError{IBPM_ERR_INVALID, why};
+        }
+        for (int k = 0; k < 2; ++k)
+            if (!tc_mult[k]) {
+                tc_mult[k] = dalloc<float>((size_t)nx * nx);
+                tc_mult_table(k == 0 ? MULT_LAPINV : MULT_AIMPL, 1, tc_mult[k]);
+            }
+    }
+    void tc_mult_table(int mode, int level, float *tab) {
+        tc_mult_kernel<<<dim3((nx + 127) / 128, nx), 128, 0, st>>>(mult(mode, level, 0), nx, tab);
+        check_launch();
+    }
+    // One batched solve x = S(m S(b)) on the tensor cores: b from the solve's
+    // prologue `in` (the first X pass's input), x to out (batch stride bs)
+    template <class In>
+    void tc_solve(const In &in, int nf, const float *mtab, double *out, long long bs) {
+        if (!tc || tc_fmax(tc) < nf) throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms not prepared"};
+        const int pe = prof_begin();
+        tc_lines_kernel<In><<<dim3(1, nx, nf), nx / 8, 0, st>>>(in, nx, tc_in_hi(tc), tc_in_lo(tc));
+        check_launch();
+        launches += tc_solve_tail(tc, nf, mtab, out, bs, nx - 1, err + 4, st);
+        CK(cudaGetLastError());
+        prof_end(pe, IBPM_KCLASS_TCDST, 16.0 * (double)ng * nf);
+    }
+
     // vort2flux (src/fluid.jl:178-205) over nbatch independent fields.
     // G, psi: level 1 of batch 0, level stride ng, batch stride bs.
     // qout: level 1 of batch 0 (level stride nq, batch stride qbs); curl_all=false
@@ -719,12 +782,24 @@ struct Engine final : ibpm_handle {
                 check_launch();
                 continue;
             }
-            if (lev == L)
-                xpass(in_plain(Gl, bs), out_plain(t1, ng), nbatch);
-            else
-                xpass(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, out_plain(t1, ng), nbatch);
-            ypass(t1, t2, ng, nbatch, mult(MULT_LAPINV, 1, 0));
-            xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch, lev == 1 ? win : nullptr);
+            bool solved = false;
+            if constexpr (std::is_same<T, double>::value) {
+                if (tc_on) {
+                    if (lev == L)
+                        tc_solve(in_plain(Gl, bs), nbatch, tc_mult[0], Pl, bs);
+                    else
+                        tc_solve(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, nbatch, tc_mult[0], Pl, bs);
+                    solved = true;
+                }
+            }
+            if (!solved) {
+                if (lev == L)
+                    xpass(in_plain(Gl, bs), out_plain(t1, ng), nbatch);
+                else
+                    xpass(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, out_plain(t1, ng), nbatch);
+                ypass(t1, t2, ng, nbatch, mult(MULT_LAPINV, 1, 0));
+                xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch, lev == 1 ? win : nullptr);
+            }
             if (curl_all || lev == 1) {
                 const dim3 blk(64, 4);
                 const dim3 grd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, nbatch);
@@ -748,12 +823,21 @@ struct Engine final : ibpm_handle {
     void apply_B(const double *z, double *x, long long xs, int nbatch) {
         reg_patch(z, nbatch);
         InRegRot<T> in{Patch<T>{patch, P.bbox, patch_stride}};
-        xpass(in, out_plain(t1, ng), nbatch, P.bbox, 1);  // rot of the patch: zero outside its rows
-        ypass(t1, t2, ng, nbatch, mult(MULT_AIMPL, 1, 0));
-        // Gw's levels 2..L hold the level-1 vorticity coarsified and zeros elsewhere:
-        // vort2flux's coarsify rewrites their central block, and nothing else ever
-        // writes them, so the zeros of the allocation stay
-        xpass(in_plain(t2, ng), out_plain(Gw, ng * L), nbatch);
+        bool solved = false;
+        if constexpr (std::is_same<T, double>::value) {
+            if (tc_on) {
+                tc_solve(in, nbatch, tc_mult[1], Gw, ng * L);
+                solved = true;
+            }
+        }
+        if (!solved) {
+            xpass(in, out_plain(t1, ng), nbatch, P.bbox, 1);  // rot of the patch: zero outside its rows
+            ypass(t1, t2, ng, nbatch, mult(MULT_AIMPL, 1, 0));
+            // Gw's levels 2..L hold the level-1 vorticity coarsified and zeros elsewhere:
+            // vort2flux's coarsify rewrites their central block, and nothing else ever
+            // writes them, so the zeros of the allocation stay
+            xpass(in_plain(t2, ng), out_plain(Gw, ng * L), nbatch);
+        }
         vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false, false, P.bbox);  // E reads the bbox only
         launch_regT(P, qw, nq, x, xs, nbatch, 0, prm, g, st);
         check_launch();
@@ -815,6 +899,7 @@ struct Engine final : ibpm_handle {
     void get_field(int field, int level, double *out) override;
     double *field_d = nullptr;  // one level of an output field
     void set_warm_start(ibpm_net *net, int mode, int depth) override;
+    void set_rebuild_transform(int products) override;
     void warm_start_sample(float *features, float *target, float *prediction) override;
     void get_state(ibpm_state_view *s) override;
     bool advance(int64_t nsteps, const ibpm_step_params *params) override;
@@ -965,7 +1050,7 @@ void Engine<T>::setup() {
     P.pc = dalloc<int>(2 * np);
     P.w = dalloc<double>((size_t)np * 2 * 49);
     P.bbox = dalloc<int>(4);
-    err = dalloc<int>(4);
+    err = dalloc<int>(8);
     P.err = err;
     ref_xb_d = dalloc<double>(2 * np);
     ds = dalloc<double>(np);
@@ -983,7 +1068,7 @@ void Engine<T>::setup() {
     prm_h = stage_prm[0];
     motion_h = stage_motion[0];
     CK(cudaMallocHost(&cg_s_h, sizeof(double) * 8));
-    CK(cudaMallocHost(&err_h, sizeof(int) * 4));
+    CK(cudaMallocHost(&err_h, sizeof(int) * 8));
     memset(prm_h, 0, sizeof(StepDev));
     CK(cudaMemcpyAsync(ref_xb_d, ref_xb.data(), sizeof(double) * 2 * np, cudaMemcpyHostToDevice, st));
 
@@ -1097,12 +1182,20 @@ void Engine<T>::build_Binv() {
 template <class T>
 void Engine<T>::assemble_invert_B() {
     const int n = 2 * np;
-    for (int c0 = 0; c0 < n; c0 += kbatch) {
-        const int nb = std::min(kbatch, n - c0);
-        unit_columns_kernel<<<(n * nb + 255) / 256, 256, 0, st>>>(fcol, n, c0, nb);
-        check_launch();
-        apply_B(fcol, Binv + (size_t)c0 * n, n, nb);
+    // the preconditioned modes may assemble with the tensor-core transforms
+    tc_on = tc_prod > 0 && preconditioned() && tc != nullptr;
+    try {
+        for (int c0 = 0; c0 < n; c0 += kbatch) {
+            const int nb = std::min(kbatch, n - c0);
+            unit_columns_kernel<<<(n * nb + 255) / 256, 256, 0, st>>>(fcol, n, c0, nb);
+            check_launch();
+            apply_B(fcol, Binv + (size_t)c0 * n, n, nb);
+        }
+    } catch (...) {
+        tc_on = false;
+        throw;
     }
+    tc_on = false;
     // n = 2 np is even: n / 2 two-step launches; after an odd count the result is in Bwork
     int m = 0;
     for (int k = 0; k < n; k += 2, ++m) {
@@ -1118,6 +1211,7 @@ void Engine<T>::assemble_invert_B() {
 // captured on first use (its buffers stay fixed until drop_graphs).
 template <class T>
 void Engine<T>::direct_rebuild() {
+    if (tc_prod > 0 && preconditioned()) tc_prepare(kbatch, tc_prod);
     if (!use_graphs || prof) {
         assemble_invert_B();
         return;
@@ -1405,6 +1499,7 @@ void Engine<T>::cg_collect() {
     CK(cudaMemcpyAsync(err_h + 2, cg_it, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(err_h + 3, err + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (uses_binv_start()) CK(cudaMemcpyAsync(err_h + 1, err + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (tc) CK(cudaMemcpyAsync(err_h + 4, err + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     cg_pending = false;
     last_cg_iters = err_h[2];
@@ -1423,6 +1518,11 @@ void Engine<T>::cg_collect() {
     if (err_h[3]) {
         CK(cudaMemsetAsync(err + 2, 0, sizeof(int), st));
         throw ApiError{IBPM_ERR_NONFINITE, "non-finite residual in CG"};
+    }
+    if (tc && err_h[4]) {
+        err_h[4] = 0;
+        CK(cudaMemsetAsync(err + 4, 0, sizeof(int), st));
+        throw ApiError{IBPM_ERR_CUDA, "a tensor-core transform pass gave up waiting for its operands"};
     }
 }
 
@@ -1890,6 +1990,29 @@ void Engine<T>::get_field(int field, int level, double *out) {
 }
 
 template <class T>
+void Engine<T>::set_rebuild_transform(int products) {
+    CK(cudaSetDevice(device));
+    if (products != 0 && products != 1 && products != 3)
+        throw ApiError{IBPM_ERR_INVALID, "the rebuild transform takes 0, 1 or 3 products"};
+    if (products != 0) {
+        if (!std::is_same<T, double>::value)
+            throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms serve the FP64 engine"};
+        if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the B rebuild exists for moving bodies only"};
+        if (nx != ny || (nx != 256 && nx != 512 && nx != 1024))
+            throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms need nx = ny in {256, 512, 1024}"};
+        tc_prepare(kbatch, products);
+    }
+    if (products != tc_prod) {
+        CK(cudaStreamSynchronize(st));
+        if (binv_exec) cudaGraphExecDestroy(binv_exec);
+        if (binv_graph) cudaGraphDestroy(binv_graph);
+        binv_exec = nullptr;
+        binv_graph = nullptr;
+    }
+    tc_prod = products;
+}
+
+template <class T>
 void Engine<T>::set_warm_start(ibpm_net *net, int mode, int depth) {
     CK(cudaSetDevice(device));
     if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the warm start applies to moving bodies (CG) only"};
@@ -2121,10 +2244,31 @@ void Engine<T>::read_profile(int kclass, int64_t *launches_out, double *ms, doub
 
 template <class T>
 void Engine<T>::diag_solve(int op, int level, const double *b, double *x) {
-    if (op < 0 || op > 2 || level < 1 || level > L) throw ApiError{IBPM_ERR_INVALID, "bad diag_solve arguments"};
+    if (op < 0 || op > 8 || level < 1 || level > L) throw ApiError{IBPM_ERR_INVALID, "bad diag_solve arguments"};
     CK(cudaSetDevice(device));
+    const int mode = op % 3 == 0 ? MULT_LAPINV : (op % 3 == 1 ? MULT_AEXPL : MULT_AIMPL);
+    if (op >= 3) {
+        if constexpr (std::is_same<T, double>::value) {
+            tc_prepare(1, op < 6 ? 1 : 3);
+            if (!tc_mult[2]) tc_mult[2] = dalloc<float>((size_t)nx * nx);
+            tc_mult_table(mode, level, tc_mult[2]);
+            double *bd = staging((size_t)ng);
+            CK(cudaMemcpyAsync(bd, b, sizeof(double) * ng, cudaMemcpyHostToDevice, st));
+            tc_solve(InPlain<double>{bd, ng, nx - 1}, 1, tc_mult[2], rhs, ng);
+            CK(cudaMemcpyAsync(x, rhs, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(err_h + 4, err + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (err_h[4]) {
+                err_h[4] = 0;
+                CK(cudaMemsetAsync(err + 4, 0, sizeof(int), st));
+                throw ApiError{IBPM_ERR_CUDA, "a tensor-core transform pass gave up waiting for its operands"};
+            }
+            return;
+        } else {
+            throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms serve the FP64 engine"};
+        }
+    }
     upload(rhs, b, (size_t)ng);
-    const int mode = op == 0 ? MULT_LAPINV : (op == 1 ? MULT_AEXPL : MULT_AIMPL);
     xpass(in_plain(rhs, ng), out_plain(t1, ng), 1);
     ypass(t1, t2, ng, 1, mult(mode, level, 0));
     xpass(in_plain(t2, ng), out_plain(rhs, ng), 1);
@@ -2654,6 +2798,11 @@ void ibpm_destroy(ibpm_handle *h) { delete h; }
 int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t depth) {
     if (!h) return IBPM_ERR_INVALID;
     return guarded(h, [&] { h->set_warm_start(net, mode, depth); });
+}
+
+int ibpm_set_rebuild_transform(ibpm_handle *h, int32_t products) {
+    if (!h) return IBPM_ERR_INVALID;
+    return guarded(h, [&] { h->set_rebuild_transform(products); });
 }
 
 int ibpm_warm_start_sample(ibpm_handle *h, float *features, float *target, float *prediction) {

@@ -194,7 +194,9 @@ class GpuCnabSolver(AbstractSolver):
         return n.value, ms.value, b.value
 
     def diag_solve(self, op: int, level: int, b: np.ndarray) -> np.ndarray:
-        """One DST-diagonalised solve on the device: op 0 Δinv, 1 A, 2 Ainv (at `level`)."""
+        """One DST-diagonalised solve on the device: op 0 Δinv, 1 A, 2 Ainv (at
+        `level`); op 3..5 the same with the tensor-core transforms of one BF16
+        product, 6..8 with three (split BF16)."""
         b = np.asfortranarray(b, dtype=np.float64)
         x = np.empty_like(b, order="F")
         _abi.check(self.lib, self._h, self.lib.ibpm_diag_solve(self._h, op, level, _abi.dptr(b), _abi.dptr(x)))
@@ -253,6 +255,13 @@ class GpuCnabSolver(AbstractSolver):
         _abi.check(self.lib, self._h, self.lib.ibpm_set_warm_start(self._h, m, net.handle if net is not None else None,
                                                                     depth))
         self._warm_net = net
+
+    def set_rebuild_transform(self, products: int):
+        """How the preconditioned modes assemble the B they invert: 0 with the
+        step's FP64 transforms, 1 or 3 with dense DST-I passes on the tensor
+        cores (one BF16 product, or three on split BF16 operands).  CG runs to
+        the same tolerance either way."""
+        _abi.check(self.lib, self._h, self.lib.ibpm_set_rebuild_transform(self._h, int(products)))
 
     def warm_start_sample(self, prediction: bool = False):
         """(features [10][np], target [2][np]) of the last step: the warm start's

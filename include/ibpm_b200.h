@@ -207,7 +207,8 @@ int64_t ibpm_kernel_launches(const ibpm_handle *h);
 #define IBPM_KCLASS_CURL 3          /* curl of the streamfunction */
 #define IBPM_KCLASS_XTRIAL 4        /* trial solve, first X pass (all levels) */
 #define IBPM_KCLASS_YTRIAL 5        /* trial solve, Y pass with the A/Ainv multiplies (all levels) */
-#define IBPM_KCLASS_COUNT 6
+#define IBPM_KCLASS_TCDST 6         /* a batched 2D solve on the tensor cores (its five launches) */
+#define IBPM_KCLASS_COUNT 7
 int ibpm_profile(ibpm_handle *h, int enable);
 int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms, double *bytes);
 
@@ -215,7 +216,10 @@ int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms,
  * operator-level parity tests.
  *   ibpm_diag_solve: x = S(S(b) scale / Lambda) on one (nx-1) x (ny-1) field with
  *     op 0: Lambda = lap_eigs (Δinv_operator, fluid.jl:117-119),
- *     op 1: A at `level`, op 2: Ainv at `level` (A_operator, fluid.jl:121-134).
+ *     op 1: A at `level`, op 2: Ainv at `level` (A_operator, fluid.jl:121-134);
+ *     op 3..5: ops 0..2 with the tensor-core transforms of one BF16 product,
+ *     op 6..8: with three products (split BF16); nx = ny in {256, 512, 1024}, FP64
+ *     engine only (see ibpm_set_rebuild_transform).
  *   ibpm_diag_apply_B: x = B z (B_operator, coupling.jl:163-176), 2*npanel.
  *   ibpm_diag_binv: the precomputed B^-1 (2np x 2np, column-major); static bodies only. */
 int ibpm_diag_solve(ibpm_handle *h, int op, int level, const double *b, double *x);
@@ -313,6 +317,17 @@ const char *ibpm_net_last_error(const ibpm_net *net);   /* NULL: the last failed
  * three) steps' stale errors, which change smoothly with the body's motion. */
 #define IBPM_WS_PRECOND_EXTRAP 6
 int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t depth);
+/* How IBPM_WS_PRECONDITIONED and IBPM_WS_PRECOND_EXTRAP assemble the B they
+ * invert (the preconditioner; no counterpart in the reference).  products 0: the
+ * FP64 transforms of the step (the default); 1 or 3: every 2D solve of the
+ * assembly as four dense DST-I passes on the tensor cores (tcgen05) with BF16
+ * operands and FP32 accumulation, one product S_hi x_hi or three
+ * (S_hi x_hi + S_hi x_lo + S_lo x_hi, each operand split as hi = bf16(v),
+ * lo = bf16(v - hi)).  The preconditioner is then close to, not equal to, the
+ * inverse; CG still runs to the same tolerance, so forces are unchanged to
+ * that tolerance and only the iteration count can differ.  Moving bodies, FP64
+ * engine, nx = ny in {256, 512, 1024}, an sm_100 device; other modes ignore it. */
+int ibpm_set_rebuild_transform(ibpm_handle *h, int32_t products);
 /* The last step's warm-start features (10 x npanel floats), target (2 x
  * npanel: the converged F~b minus the extrapolated guess x_e) and, in the
  * learned mode, the network's correction as the step used it (zeros

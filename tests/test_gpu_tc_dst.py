@@ -1,0 +1,153 @@
+"""The tensor-core DST-I passes (csrc/tc_dst.cu) and the preconditioner they build.
+
+A 2D solve x = S(m ⊙ S(b)) (src/fluid.jl:145-166 with FFTW's RODFT00 as S) runs
+as four dense passes D = S X on tcgen05 with BF16 operands and FP32
+accumulation.  `_emulate` restates that arithmetic in numpy (the same splits,
+roundings and pass order; only the FP32 summation order differs), so the GPU
+result must sit on the emulation, far closer than either sits to the FP64
+solve.  The preconditioned moving-body modes then assemble B with these solves:
+CG still stops at the same tolerance, so forces agree with the FP64 rebuild to
+that tolerance, and the inverse preconditions B well."""
+import numpy as np
+import pytest
+import scipy.fft as sf
+
+pytestmark = pytest.mark.gpu
+
+CG = dict(reltol=0.0, abstol=1e-10, maxiter=5000)
+
+
+def _bf16(x):
+    x = np.asarray(x, np.float32)
+    b = x.view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32)
+
+
+def _emulate(b2, mult, nprod):
+    """The four passes on (P-1)^2 field b2 [y][x] with multipliers mult [ky][kx]."""
+    m = b2.shape[0]
+    P = m + 1
+    j = np.arange(1, P)
+    S = np.zeros((P, P))
+    S[:m, :m] = 2 * np.sin(np.pi * np.outer(j, j) / P)
+    Sh = _bf16(S)
+    Sl = _bf16(S - Sh)
+    X = np.zeros((P, P))
+    X[:m, :m] = b2
+    Xh = _bf16(X)
+    Xl = _bf16(X - Xh)
+
+    def gemm(xh, xl):  # D[k][l] = sum_p S[k][p] X[l][p]
+        D = Sh @ xh.T
+        if nprod == 3:
+            D = D + Sh @ xl.T + Sl @ xh.T
+        return D.astype(np.float32)
+
+    def split(D):
+        h = _bf16(D)
+        return h, _bf16(D - h)
+
+    D1 = gemm(Xh, Xl)
+    M = np.zeros((P, P), np.float32)
+    M[:m, :m] = mult
+    D2 = (gemm(*split(D1)) * M).astype(np.float32)
+    D4 = gemm(*split(gemm(*split(D2))))
+    return D4[:m, :m].astype(np.float64)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _plate(ib, n=256):
+    prob = ib.configs.pitching_plate(0.5, h=0.02, n=n, nlevel=3, npts=51, dt=0.004)
+    return ib.GpuCnabSolver(ib.State(prob), cg=CG)
+
+
+@pytest.mark.parametrize("n", [256, 512])
+def test_tensor_core_solve_follows_its_arithmetic(ib, n):
+    """Δinv and Ainv (level 2) of a seeded field through ibpm_diag_solve ops 3..8."""
+    s = _plate(ib, n)
+    m = n - 1
+    rng = np.random.default_rng(n)
+    b = rng.normal(size=(m, m))  # [y][x]
+    i = np.arange(1, n)
+    lam = -2 * (np.cos(np.pi * i[None, :] / n) + np.cos(np.pi * i[:, None] / n) - 2)  # [ky][kx]
+    scale = 1.0 / (4 * n * n)
+    hc = s.state.prob.fluid.grid.gridstep(2)
+    c = s.state.prob.scheme.dt / (2 * s.state.prob.fluid.Re * hc * hc)
+    mults = {0: scale / lam, 2: scale / (1 + lam * c)}
+    bf = b.T.reshape(-1, order="F")  # column-major (x fastest) field of the ABI
+    for op, mult in mults.items():
+        exact = sf.dstn(sf.dstn(b, type=1) * mult, type=1)
+        x64 = s.diag_solve(op, 2, bf).reshape(m, m, order="F").T
+        assert _rel(x64, exact) <= 1e-12
+        for nprod, bar in ((1, 1e-2), (3, 2e-5)):
+            emu = _emulate(b, mult.astype(np.float32), nprod)
+            xtc = s.diag_solve(op + (3 if nprod == 1 else 6), 2, bf).reshape(m, m, order="F").T
+            e_emu, e_gpu = _rel(emu, exact), _rel(xtc, exact)
+            assert e_gpu <= bar, (op, nprod, e_gpu)
+            assert _rel(xtc, emu) <= 0.2 * e_emu, (op, nprod, _rel(xtc, emu), e_emu)
+
+
+@pytest.mark.parametrize("products", [1, 3])
+def test_tensor_core_rebuild_preconditions_cg(ib, products):
+    """The preconditioned mode with B assembled on the tensor cores: the inverse
+    of a rebuild step against B assembled in FP64 (diag_apply_B), and 24 steps
+    whose forces match the FP64 rebuild's to the CG tolerance with about as many
+    iterations."""
+    runs = {}
+    for prod in (0, products):
+        s = _plate(ib)
+        s.set_warm_start(None, mode="preconditioned", depth=8)
+        s.set_rebuild_transform(prod)
+        it = []
+        for k in range(24):
+            s.advance_()
+            it.append(s.info().last_cg_iters)
+            if k == 16 and prod:  # a rebuild step: Binv is this step's
+                n = 2 * s.state.prob.bodies.npanel
+                B = np.stack([s.diag_apply_B(np.eye(n)[q]) for q in range(n)], axis=1)
+                lam = np.linalg.eigvals(s.diag_binv() @ B)
+                spread = np.abs(lam - 1).max()
+                assert spread <= (0.1 if products == 1 else 1e-3), spread
+        runs[prod] = (np.asarray(it), s.total_force().copy())
+        del s
+    (i0, f0), (it, f) = runs[0], runs[products]
+    assert np.abs(f - f0).max() <= 1e-6 * np.abs(f0).max()
+    assert it.mean() <= i0.mean() + (2 if products == 1 else 0.5), (it, i0)
+
+
+def test_tensor_core_rebuild_eager_matches_graph(ib):
+    """With profiling on the rebuild runs without its graph: the same iterations
+    and forces, and the tensor-core class is timed."""
+    out = {}
+    for eager in (False, True):
+        s = _plate(ib)
+        s.set_warm_start(None, mode="preconditioned_extrapolated", depth=4)
+        s.set_rebuild_transform(3)
+        if eager:
+            s.profile(True)
+        it = []
+        for _ in range(9):
+            s.advance_()
+            it.append(s.info().last_cg_iters)
+        if eager:
+            n, ms, _ = s.profile_read("tcdst")
+            assert n > 0 and ms > 0
+        out[eager] = (it, s.total_force().copy())
+        del s
+    assert out[False][0] == out[True][0]
+    assert np.abs(out[False][1] - out[True][1]).max() <= 1e-13 * np.abs(out[False][1]).max()
+
+
+def test_tensor_core_rebuild_errors(ib):
+    s = _plate(ib)
+    with pytest.raises(Exception):
+        s.set_rebuild_transform(2)
+    prob = ib.configs.pitching_plate(0.5, h=0.04, n=128, nlevel=3, npts=26, dt=0.004)
+    s2 = ib.GpuCnabSolver(ib.State(prob), cg=CG)
+    with pytest.raises(Exception):
+        s2.set_rebuild_transform(3)  # 128 x 128 is not a tensor-core size
+    s2.set_rebuild_transform(0)
