@@ -189,7 +189,9 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
     reference's start (the previous solution), the extrapolated start, the
     learned start, the projection onto the last 16 solutions, the direct start
     (B assembled and inverted on the GPU every step, or every 8th) and CG
-    preconditioned by that inverse rebuilt every 8th or 32nd step; the network is
+    preconditioned by that inverse rebuilt every 8th or 32nd step (B assembled
+    with the FP64 transforms, or on the tensor cores with three or one BF16
+    products: "tc3", "tc1"); the network is
     trained on samples of k = 0.25, 0.45, 0.65 and 0.85 generated by the solver
     (after a 60-step start-up).  Every run takes the same steps, so their final
     forces differ only by the CG tolerance."""
@@ -214,11 +216,17 @@ def warm_start_report(ib, device: int, train_steps: int = 100, eval_steps: int =
             ("projected", "projected", 16), ("direct", "direct", 1), ("direct_every_8", "direct", 8),
             ("preconditioned_every_8", "preconditioned", 8), ("preconditioned_every_32", "preconditioned", 32),
             ("preconditioned_extrapolated_every_8", "preconditioned_extrapolated", 8),
-            ("preconditioned_extrapolated_every_32", "preconditioned_extrapolated", 32))
-    for label, mode, depth in runs:
+            ("preconditioned_extrapolated_every_32", "preconditioned_extrapolated", 32),
+            ("preconditioned_extrapolated_tc3_every_8", "preconditioned_extrapolated", 8, 3),
+            ("preconditioned_extrapolated_tc3_every_32", "preconditioned_extrapolated", 32, 3),
+            ("preconditioned_extrapolated_tc1_every_8", "preconditioned_extrapolated", 8, 1),
+            ("preconditioned_extrapolated_tc1_every_32", "preconditioned_extrapolated", 32, 1))
+    for label, mode, depth, *tc in runs:
         s = make(0.55)
         if mode != "previous":
             s.set_warm_start(net if mode == "learned" else None, mode=mode, depth=depth)
+        if tc:
+            s.set_rebuild_transform(tc[0])
         for _ in range(60):  # start-up transient, excluded
             s.advance_()
         stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -313,17 +321,23 @@ def mixed_precision_plate_report(ib, device: int, steps: int = 200, timed: int =
     return out
 
 
-def direct_start_run(ib, device: int, steps: int, warmup: int, npts: int = 101):
+def direct_start_run(ib, device: int, steps: int, warmup: int, npts: int = 101, products: int = 0):
     """The direct CG start alone (B assembled and inverted on the GPU every step)
     on the 512^2 x 4-level pitching plate at k = 0.55 with `npts` points (B has
     2 npts columns): `warmup` steps, then `steps` steps timed with CUDA events on
     the solver's stream, the last of them inside the NVTX range "direct_step"
-    (the range a kernel-launch list or a profile selects)."""
+    (the range a kernel-launch list or a profile selects).  With products 1 or 3
+    the step is the preconditioned mode rebuilt every step, its B assembled on
+    the tensor cores with that many BF16 products."""
     import torch
 
     s = ib.GpuCnabSolver(ib.State(ib.configs.pitching_plate(0.55, npts=npts)),
                          cg=dict(reltol=0.0, abstol=1e-10, maxiter=5000), device=device)
-    s.set_warm_start(None, mode="direct", depth=1)
+    if products:
+        s.set_warm_start(None, mode="preconditioned", depth=1)
+        s.set_rebuild_transform(products)
+    else:
+        s.set_warm_start(None, mode="direct", depth=1)
     for _ in range(warmup):
         s.advance_()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -343,7 +357,9 @@ def direct_start_run(ib, device: int, steps: int, warmup: int, npts: int = 101):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    return {"metric": "moving-body steps/s, direct CG start", "value": 1000.0 / ms, "unit": "steps/s",
+    what = f"preconditioned CG rebuilt every step, B on the tensor cores ({products} BF16 products)" if products \
+        else "direct CG start"
+    return {"metric": f"moving-body steps/s, {what}", "value": 1000.0 / ms, "unit": "steps/s",
             "ms_per_step": ms, "steps": steps, "warmup": warmup, "cg_iterations_mean": float(np.mean(it)),
             "gpu_launches_per_step": (s.kernel_launches() - l0) / steps,
             "config": {"workload": f"pitching_plate_512: 512x512 cells x 4 levels, {npts}-point plate, Re 500, dt 0.002, "
@@ -439,13 +455,16 @@ def main():
                     help="time only the moving-body direct CG start (one JSON line) and exit")
     ap.add_argument("--direct-start-points", type=int, default=101,
                     help="plate points of --direct-start-only (B has twice as many columns)")
+    ap.add_argument("--rebuild-products", type=int, default=0, choices=[0, 1, 3],
+                    help="--direct-start-only: assemble B on the tensor cores with 1 or 3 BF16 products "
+                         "(the preconditioned mode rebuilt every step)")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
         return run_reference(args, world, rank)
     if args.direct_start_only:
         ib = load_package()
-        line = direct_start_run(ib, local, args.steps, args.warmup, args.direct_start_points)
+        line = direct_start_run(ib, local, args.steps, args.warmup, args.direct_start_points, args.rebuild_products)
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
