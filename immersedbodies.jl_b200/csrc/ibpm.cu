@@ -735,14 +735,16 @@ struct Engine final : ibpm_handle {
         check_launch();
     }
     // One batched solve x = S(m S(b)) on the tensor cores: b from the solve's
-    // prologue `in` (the first X pass's input), x to out (batch stride bs)
+    // prologue `in` (the first X pass's input), x to out (batch stride bs), the
+    // elements `keep` selects
     template <class In>
-    void tc_solve(const In &in, int nf, const float *mtab, double *out, long long bs) {
+    void tc_solve(const In &in, int nf, const float *mtab, double *out, long long bs,
+                  TcKeep keep = TcKeep{TC_KEEP_ALL, nullptr, {0, 0, 0, 0}}) {
         if (!tc || tc_fmax(tc) < nf) throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms not prepared"};
         const int pe = prof_begin();
         tc_lines_kernel<In><<<dim3(1, nx, nf), nx / 8, 0, st>>>(in, nx, tc_in_hi(tc), tc_in_lo(tc));
         check_launch();
-        launches += tc_solve_tail(tc, nf, mtab, out, bs, nx - 1, err + 4, st);
+        launches += tc_solve_tail(tc, nf, mtab, out, bs, nx - 1, keep, err + 4, st);
         CK(cudaGetLastError());
         prof_end(pe, IBPM_KCLASS_TCDST, 16.0 * (double)ng * nf);
     }
@@ -785,10 +787,14 @@ struct Engine final : ibpm_handle {
             bool solved = false;
             if constexpr (std::is_same<T, double>::value) {
                 if (tc_on) {
+                    // coarse levels: only the lines the next finer level's boundary
+                    // values read; level 1: the curl's window
+                    TcKeep keep{TC_KEEP_LINES, nullptr, {ny / 4 - 1, 3 * ny / 4 - 1, nx / 4 - 1, 3 * nx / 4 - 1}};
+                    if (lev == 1) keep = win ? TcKeep{TC_KEEP_WINDOW, win, {0, 0, 0, 0}} : TcKeep{TC_KEEP_ALL, nullptr, {0, 0, 0, 0}};
                     if (lev == L)
-                        tc_solve(in_plain(Gl, bs), nbatch, tc_mult[0], Pl, bs);
+                        tc_solve(in_plain(Gl, bs), nbatch, tc_mult[0], Pl, bs, keep);
                     else
-                        tc_solve(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, nbatch, tc_mult[0], Pl, bs);
+                        tc_solve(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, nbatch, tc_mult[0], Pl, bs, keep);
                     solved = true;
                 }
             }

@@ -1,15 +1,11 @@
 // Dense DST-I passes on the fifth-generation tensor cores (see tc_dst.h).
 //
-// One CTA computes a 128 x 256 tile D[k][l] (k: 128 output frequencies = rows of
-// S, l: 256 lines of one field) over the whole line length P, accumulating in
-// 256 columns of tensor memory.  Thread roles in the 128-thread CTA:
-//   warp 0, one lane: TMA producer, K-blocks of 64 elements (128 B rows, 128-byte
-//     swizzle) of S (hi, lo) and of the lines (hi, lo) into a ring of stages;
-//   warp 1, one lane: issues tcgen05.mma (M 128, N 256, K 16; BF16 x BF16 -> FP32)
-//     for every K-block, and tcgen05.commit frees a stage when its products are done;
-//   warp 2: allocates and frees the tensor memory;
-//   all four warps: the epilogue, each warp reading its 32 lanes (rows k) with
-//     tcgen05.ld, and writing row k of the next pass's lines (rows become lines).
+// A tile is D[k][l] for 128 output frequencies k (rows of S) and 256 lines l of
+// one field over the whole line length P, accumulated in 256 columns of tensor
+// memory by tcgen05.mma (M 128, N 256, K 16; BF16 x BF16 -> FP32) from K-blocks
+// of 64 elements (128-byte rows, 128-byte swizzle) that TMA brings into a ring
+// of shared-memory stages; the epilogue reads its rows with tcgen05.ld and
+// writes row k as line k of the next pass (rows become lines).
 // Every wait on an mbarrier gives up after one second of global time, sets the
 // caller's error flag and lets the CTA finish (freeing its tensor memory); no wait
 // depends on another CTA.  No load here uses cluster-wide delivery.
@@ -27,7 +23,6 @@ namespace {
 constexpr int kTileM = 128;   // rows of S per CTA
 constexpr int kTileN = 256;   // lines per CTA
 constexpr int kBlockK = 64;   // elements per K-block: one 128-byte swizzle row
-constexpr int kThreads = 128;
 constexpr uint32_t kTmemCols = 256;
 constexpr int kBytesA = kTileM * kBlockK * 2;  // 16 KB
 constexpr int kBytesB = kTileN * kBlockK * 2;  // 32 KB
@@ -39,7 +34,8 @@ struct Cfg {
     static constexpr int kParts = NPROD == 3 ? 2 : 1;
     static constexpr int kStageBytes = kParts * (kBytesA + kBytesB);
     static constexpr int kStages = NPROD == 3 ? 2 : 4;
-    static constexpr size_t kSmem = (size_t)kStages * kStageBytes + 1024;  // + alignment slack
+    // the operand ring, four epilogue staging tiles and alignment slack
+    static constexpr size_t kSmem = (size_t)kStages * kStageBytes + 4 * 32 * 33 * sizeof(float) + 1024;
 };
 
 struct PassArgs {
@@ -49,8 +45,18 @@ struct PassArgs {
     double *out;              // result (EPI_F64)
     long long bs;
     int ld;
+    TcKeep keep;              // which result elements are stored (EPI_F64)
     int *err;
 };
+
+// 0-based (x, y) of the result: stored or not
+__device__ __forceinline__ bool kept(const TcKeep &k, int x, int y) {
+    if (k.mode == TC_KEEP_WINDOW)
+        return x >= k.win[0] - 2 && x <= k.win[1] && y >= k.win[2] - 2 && y <= k.win[3];
+    if (k.mode == TC_KEEP_LINES)
+        return y == k.lines[0] || y == k.lines[1] || x == k.lines[2] || x == k.lines[3];
+    return true;
+}
 
 __device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -143,34 +149,104 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Rows row0 .. row0 + 31 of a tile (one warp, lane = row), columns col0 .. col0
+// + 31 (v: FP32 bits from tensor memory): multiplied (EPI_MULT), then stored as
+// the next pass's BF16 parts (EPI_SPLIT, EPI_MULT) or as the FP64 result
+// (EPI_F64: interior elements that the selection keeps).  The warp's staging
+// tile stg (32 x 33 floats, conflict-free both ways) turns the stores into
+// coalesced 64-byte (BF16) and 256-byte (FP64) row segments.
+constexpr int kStageLd = 33;
+constexpr int kStageFloats = 32 * kStageLd;
+
+template <int NPROD, int EPI>
+__device__ __forceinline__ void epilogue_staged(const PassArgs &a, int f, int row0, int col0, const uint32_t (&v)[32],
+                                                float *stg) {
+    const int lane = threadIdx.x & 31, P = a.P;
+    float x[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) x[j] = __uint_as_float(v[j]);
+    if (EPI == EPI_MULT) {
+        const float4 *mp = reinterpret_cast<const float4 *>(a.mult + (size_t)(row0 + lane) * P + col0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 m = __ldg(mp + q);
+            x[4 * q] *= m.x;
+            x[4 * q + 1] *= m.y;
+            x[4 * q + 2] *= m.z;
+            x[4 * q + 3] *= m.w;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) stg[lane * kStageLd + j] = x[j];
+    __syncwarp();
+    if (EPI == EPI_F64) {
+        const int col = col0 + lane;
+        double *o = a.out + (long long)f * a.bs + col;
+        for (int r = 0; r < 32; ++r) {
+            const int row = row0 + r;
+            if (row < P - 1 && col < P - 1 && kept(a.keep, col, row))
+                o[(long long)row * a.ld] = (double)stg[r * kStageLd + lane];
+        }
+    } else {
+        const int q = lane & 3;
+#pragma unroll
+        for (int it = 0; it < 4; ++it) {
+            const int r = it * 8 + (lane >> 2);
+            __align__(16) __nv_bfloat16 h[8];
+            __align__(16) __nv_bfloat16 l[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) tc_split(stg[r * kStageLd + 8 * q + i], h[i], l[i]);
+            const size_t off = ((size_t)f * P + row0 + r) * P + col0 + 8 * q;
+            *reinterpret_cast<uint4 *>(a.oh + off) = *reinterpret_cast<const uint4 *>(h);
+            if (NPROD == 3) *reinterpret_cast<uint4 *>(a.ol + off) = *reinterpret_cast<const uint4 *>(l);
+        }
+    }
+    __syncwarp();
+}
+
+// One CTA per SM walks the tiles (M-tiles fastest, so the CTAs working at once
+// share each line tile through L2).  Two accumulators of
+// 256 tensor-memory columns let the epilogue of one tile run while the products
+// of the next accumulate.  Warps: 0 producer (one lane), 1 products (one lane;
+// the whole warp allocates and frees the 512 columns), 2..5 epilogue (warp w
+// reads lanes 32 (w % 4) ..).
+constexpr int kThreads = 192;
+
 template <int NPROD, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_dst_pass_kernel(const __grid_constant__ CUtensorMap tSh, const __grid_constant__ CUtensorMap tSl,
-                       const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl, PassArgs a) {
+                             const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl,
+                             PassArgs a, int nf) {
     using C = Cfg<NPROD>;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t full[C::kStages], empty[C::kStages], done;
+    __shared__ uint64_t full[C::kStages], empty[C::kStages], accf[2], acce[2], fin;
     __shared__ uint32_t tmem_s;
     __shared__ int fail_s;
-    // the 128-byte swizzle atoms must start on 1024-byte boundaries of the shared window
     uint8_t *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN, f = blockIdx.z;
-    const int P = a.P, KB = P / kBlockK;
+    const int P = a.P, KB = P / kBlockK, MT = P / kTileM, NT = P / kTileN;
+    // epilogue warp w (2..5) stages through its own tile after the operand ring
+    float *stg = reinterpret_cast<float *>(smem + (size_t)C::kStages * C::kStageBytes) +
+                 (warp >= 2 ? (warp - 2) * kStageFloats : 0);
+    const int ntiles = nf * MT * NT;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::kStages; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&done, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], 128);
+        }
+        mbar_init(&fin, 1);
         fail_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    if (warp == 2) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&tmem_s)),
-                     "r"(kTmemCols)
+                     "r"(2 * kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -184,103 +260,102 @@ __global__ void __launch_bounds__(kThreads, 1)
         return smem + (size_t)s * C::kStageBytes + C::kParts * kBytesA + part * kBytesB;
     };
 
-    if (warp == 0 && lane == 0) {
-        for (int kb = 0; kb < KB; ++kb) {
-            const int s = kb % C::kStages;
-            if (kb >= C::kStages && !mbar_wait(&empty[s], ((kb / C::kStages) - 1) & 1)) {
-                atomicExch(&fail_s, 1);
-                break;
-            }
-            mbar_expect_tx(&full[s], C::kStageBytes);
-            const int x = kb * kBlockK;
-            tma_load(stage_a(s, 0), &tSh, &full[s], x, m0);
-            tma_load(stage_b(s, 0), &tXh, &full[s], x, f * P + n0);
-            if (NPROD == 3) {
-                tma_load(stage_a(s, 1), &tSl, &full[s], x, m0);
-                tma_load(stage_b(s, 1), &tXl, &full[s], x, f * P + n0);
-            }
-        }
-    } else if (warp == 1 && lane == 0) {
-        for (int kb = 0; kb < KB; ++kb) {
-            const int s = kb % C::kStages;
-            if (!mbar_wait(&full[s], (kb / C::kStages) & 1)) {
-                atomicExch(&fail_s, 1);
-                break;
-            }
-            tc_fence_after();
-            const uint64_t ah = sw128_desc(saddr(stage_a(s, 0))), bh = sw128_desc(saddr(stage_b(s, 0)));
-            const uint64_t al = sw128_desc(saddr(stage_a(s, NPROD == 3 ? 1 : 0)));
-            const uint64_t bl = sw128_desc(saddr(stage_b(s, NPROD == 3 ? 1 : 0)));
-#pragma unroll
-            for (int kk = 0; kk < kBlockK / 16; ++kk) {
-                const uint64_t o = (uint64_t)(kk * 32 >> 4);  // 16 elements = 32 B along the swizzled row
-                mma(tmem, ah + o, bh + o, (kb | kk) != 0);
-                if (NPROD == 3) {
-                    mma(tmem, ah + o, bl + o, 1);
-                    mma(tmem, al + o, bh + o, 1);
+    if (warp == 0) {
+        if (lane == 0) {
+            int kc = 0;  // K-blocks loaded so far (the ring position)
+            for (int t = blockIdx.x; t < ntiles && !fail_s; t += gridDim.x) {
+                const int m0 = (t % MT) * kTileM, n0 = ((t / MT) % NT) * kTileN, f = t / (MT * NT);
+                for (int kb = 0; kb < KB; ++kb, ++kc) {
+                    const int s = kc % C::kStages;
+                    if (kc >= C::kStages && !mbar_wait(&empty[s], ((kc / C::kStages) - 1) & 1)) {
+                        atomicExch(&fail_s, 1);
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], C::kStageBytes);
+                    const int x = kb * kBlockK;
+                    tma_load(stage_a(s, 0), &tSh, &full[s], x, m0);
+                    tma_load(stage_b(s, 0), &tXh, &full[s], x, f * P + n0);
+                    if (NPROD == 3) {
+                        tma_load(stage_a(s, 1), &tSl, &full[s], x, m0);
+                        tma_load(stage_b(s, 1), &tXl, &full[s], x, f * P + n0);
+                    }
                 }
             }
-            mma_commit(&empty[s]);
         }
-        mma_commit(&done);  // arrives once every product issued above has completed
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int kc = 0, i = 0;
+            for (int t = blockIdx.x; t < ntiles && !fail_s; t += gridDim.x, ++i) {
+                const int b = i & 1, u = i >> 1;
+                if (u >= 1 && !mbar_wait(&acce[b], (u - 1) & 1)) {
+                    atomicExch(&fail_s, 1);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t acc = tmem + (uint32_t)(b * kTmemCols);
+                bool ok = true;
+                for (int kb = 0; kb < KB; ++kb, ++kc) {
+                    const int s = kc % C::kStages;
+                    if (!mbar_wait(&full[s], (kc / C::kStages) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t ah = sw128_desc(saddr(stage_a(s, 0))), bh = sw128_desc(saddr(stage_b(s, 0)));
+                    const uint64_t al = sw128_desc(saddr(stage_a(s, NPROD == 3 ? 1 : 0)));
+                    const uint64_t bl = sw128_desc(saddr(stage_b(s, NPROD == 3 ? 1 : 0)));
+#pragma unroll
+                    for (int kk = 0; kk < kBlockK / 16; ++kk) {
+                        const uint64_t o = (uint64_t)(kk * 32 >> 4);
+                        mma(acc, ah + o, bh + o, (kb | kk) != 0);
+                        if (NPROD == 3) {
+                            mma(acc, ah + o, bl + o, 1);
+                            mma(acc, al + o, bh + o, 1);
+                        }
+                    }
+                    mma_commit(&empty[s]);
+                }
+                mma_commit(&accf[b]);  // the tile's products (or those issued before a failure)
+                if (!ok) {
+                    atomicExch(&fail_s, 1);
+                    break;
+                }
+            }
+            // every product issued here has finished before the columns are freed
+            mma_commit(&fin);
+            if (!mbar_wait(&fin, 0)) atomicExch(&fail_s, 1);
+        }
+    } else {
+        const int q = warp & 3;  // the lane quarter this warp may read
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+            const int b = i & 1, u = i >> 1;
+            const bool ok = mbar_wait(&accf[b], u & 1);
+            tc_fence_after();
+            // one decision per warp: the tensor-memory loads below are warp-wide
+            if (__any_sync(0xffffffffu, !ok || fail_s)) {
+                atomicExch(&fail_s, 1);
+                break;
+            }
+            const int m0 = (t % MT) * kTileM, n0 = ((t / MT) % NT) * kTileN, f = t / (MT * NT);
+            const uint32_t acc = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTmemCols);
+            for (int c = 0; c < kTileN; c += 32) {
+                uint32_t v[32];
+                tmem_ld32(acc + (uint32_t)c, v);
+                epilogue_staged<NPROD, EPI>(a, f, m0 + q * 32, n0 + c, v, stg);
+            }
+            tc_fence_before();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(&acce[b])) : "memory");
+        }
     }
     __syncwarp();
-
-    const bool ok = mbar_wait(&done, 0);
-    tc_fence_after();
-    if (!ok) atomicExch(&fail_s, 1);
-    __syncthreads();
-    if (fail_s) {
-        if (threadIdx.x == 0) atomicExch(a.err, 1);
-    } else {
-        const int row = m0 + warp * 32 + lane;  // output frequency (or position) index
-        for (int c = 0; c < kTileN; c += 32) {
-            uint32_t v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-            const int col0 = n0 + c;
-            float x[32];
-#pragma unroll
-            for (int j = 0; j < 32; ++j) x[j] = __uint_as_float(v[j]);
-            if (EPI == EPI_MULT) {
-                const float4 *mp = reinterpret_cast<const float4 *>(a.mult + (size_t)row * P + col0);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const float4 m = __ldg(mp + q);
-                    x[4 * q] *= m.x;
-                    x[4 * q + 1] *= m.y;
-                    x[4 * q + 2] *= m.z;
-                    x[4 * q + 3] *= m.w;
-                }
-            }
-            if (EPI == EPI_F64) {
-                if (row < P - 1) {
-                    double *o = a.out + (long long)f * a.bs + (long long)row * a.ld + col0;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        if (col0 + j < P - 1) o[j] = (double)x[j];
-                }
-            } else {
-                __align__(16) __nv_bfloat16 h[32];
-                __align__(16) __nv_bfloat16 l[32];
-#pragma unroll
-                for (int j = 0; j < 32; ++j) tc_split(x[j], h[j], l[j]);
-                const size_t off = ((size_t)f * P + row) * P + col0;
-                uint4 *oh = reinterpret_cast<uint4 *>(a.oh + off);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) oh[q] = reinterpret_cast<const uint4 *>(h)[q];
-                if (NPROD == 3) {
-                    uint4 *ol = reinterpret_cast<uint4 *>(a.ol + off);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) ol[q] = reinterpret_cast<const uint4 *>(l)[q];
-                }
-            }
-        }
-    }
     tc_fence_before();
     __syncthreads();
-    if (warp == 2) {
+    if (fail_s && threadIdx.x == 0) atomicExch(a.err, 1);
+    if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTmemCols)
+                     : "memory");
     }
 }
 
@@ -339,7 +414,7 @@ bool set_smem_attr() {
 }  // namespace
 
 struct TcDstPlan {
-    int P = 0, fmax = 0, nprod = 1;
+    int P = 0, fmax = 0, nprod = 1, nsm = 148;
     __nv_bfloat16 *S[2] = {nullptr, nullptr};
     __nv_bfloat16 *X[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [buffer][hi, lo]
     CUtensorMap mS[2], mX[2][2];
@@ -370,6 +445,7 @@ TcDstPlan *tc_create(int P, int fmax, int nprod, const char **why) {
     if (prop.major != 10 || prop.minor != 0) return fail(nullptr, "tensor-core transforms are built for sm_100a");
     if (!encoder()) return fail(nullptr, "cuTensorMapEncodeTiled is unavailable");
     TcDstPlan *p = new TcDstPlan;
+    p->nsm = prop.multiProcessorCount;
     p->P = P;
     p->fmax = fmax;
     p->nprod = nprod;
@@ -420,19 +496,20 @@ __nv_bfloat16 *tc_in_lo(TcDstPlan *p) { return p->nprod == 3 ? p->X[0][1] : null
 
 template <int NPROD>
 static void tc_pass(TcDstPlan *p, int src, int epi, int nf, PassArgs a, cudaStream_t st) {
-    const dim3 grid(p->P / kTileM, p->P / kTileN, nf);
-    const size_t sm = Cfg<NPROD>::kSmem;
     const CUtensorMap &sh = p->mS[0], &sl = p->mS[1], &xh = p->mX[src][0], &xl = p->mX[src][1];
+    const int ntiles = nf * (p->P / kTileM) * (p->P / kTileN);
+    const int g = ntiles < p->nsm ? ntiles : p->nsm;
+    const size_t sm = Cfg<NPROD>::kSmem;
     if (epi == EPI_SPLIT)
-        tc_dst_pass_kernel<NPROD, EPI_SPLIT><<<grid, kThreads, sm, st>>>(sh, sl, xh, xl, a);
+        tc_dst_pass_kernel<NPROD, EPI_SPLIT><<<g, kThreads, sm, st>>>(sh, sl, xh, xl, a, nf);
     else if (epi == EPI_MULT)
-        tc_dst_pass_kernel<NPROD, EPI_MULT><<<grid, kThreads, sm, st>>>(sh, sl, xh, xl, a);
+        tc_dst_pass_kernel<NPROD, EPI_MULT><<<g, kThreads, sm, st>>>(sh, sl, xh, xl, a, nf);
     else
-        tc_dst_pass_kernel<NPROD, EPI_F64><<<grid, kThreads, sm, st>>>(sh, sl, xh, xl, a);
+        tc_dst_pass_kernel<NPROD, EPI_F64><<<g, kThreads, sm, st>>>(sh, sl, xh, xl, a, nf);
 }
 
-int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long long bs, int ld, int *err,
-                  cudaStream_t st) {
+int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long long bs, int ld, TcKeep keep,
+                  int *err, cudaStream_t st) {
     if (nf < 1 || nf > p->fmax) return -1;
     PassArgs a{};
     a.P = p->P;
@@ -440,6 +517,7 @@ int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long lon
     a.out = out;
     a.bs = bs;
     a.ld = ld;
+    a.keep = keep;
     a.err = err;
     // (y, x) -> (kx, y) -> (ky, kx) [x m] -> (x, ky) -> (y, x)
     const int epis[4] = {EPI_SPLIT, EPI_MULT, EPI_SPLIT, EPI_F64};

@@ -31,13 +31,25 @@ int tc_fmax(const TcDstPlan *p);
 // the buffer the first pass reads: [f][line y][position x], P x P per field
 __nv_bfloat16 *tc_in_hi(TcDstPlan *p);
 __nv_bfloat16 *tc_in_lo(TcDstPlan *p);
+// Which elements of the result a solve stores: all; those a windowed curl
+// reads (win: device [i0, i1, j0, j1], 1-based face indices; the psi entries
+// (i - 1 .. i, j - 1 .. j) of every face in it); or the four lines a finer
+// level's boundary values read (lines: 0-based rows y0, y1 and columns x0, x1).
+enum { TC_KEEP_ALL = 0, TC_KEEP_WINDOW = 1, TC_KEEP_LINES = 2 };
+struct TcKeep {
+    int mode;
+    const int *win;
+    int lines[4];
+};
+
 // Runs the four passes over nf fields whose lines the caller wrote to
 // tc_in_hi / tc_in_lo; mult (device, P x P floats, [ky][kx]) is applied after
-// the second pass; the result goes to out[f * bs + x + ld * y] for x, y < P - 1.
-// *err (device) is set to 1 if a wait inside a pass gave up (after one second;
-// never in normal use).  Returns the number of kernels launched.
-int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long long bs, int ld, int *err,
-                  cudaStream_t st);
+// the second pass; the result goes to out[f * bs + x + ld * y] for x, y < P - 1
+// that `keep` selects.  *err (device) is set to 1 if a wait inside a pass gave
+// up (after one second; never in normal use).  Returns the number of kernels
+// launched.
+int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long long bs, int ld, TcKeep keep,
+                  int *err, cudaStream_t st);
 
 // Splits v into hi = bf16(v), lo = bf16(v - hi).
 __device__ __forceinline__ void tc_split(float v, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
