@@ -41,12 +41,15 @@ namespace {
 constexpr int kNG = 2;  // FFT groups (line pairs) per block
 
 // Spectral multipliers of one level for the tensor-core transforms, as FP32
-// [ky][kx] (P x P, zero in the padding row and column)
+// [kx][ky] with both frequencies in the transforms' block order (P x P, zero at
+// the padding slots)
 __global__ void tc_mult_kernel(Mult m, int P, float *tab) {
-    const int kx = blockIdx.x * blockDim.x + threadIdx.x, ky = blockIdx.y;
-    if (kx >= P) return;
-    tab[(size_t)ky * P + kx] = (kx < P - 1 && ky < P - 1) ? (float)m(m.coef(0), kx + 1, ky + 1) : 0.0f;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    if (r >= P) return;
+    const int kx = tc_blk(c, P), ky = tc_blk(r, P);
+    tab[(size_t)c * P + r] = (kx != 0 && ky != 0) ? (float)m(m.coef(0), kx, ky) : 0.0f;
 }
+
 constexpr int kNGWide = 4, kWideBatch = 16;  // Y-pass groups per block for launches over >= kWideBatch fields
 
 thread_local std::string g_create_error;
@@ -298,8 +301,8 @@ struct Engine final : ibpm_handle {
     int *ws_nvalid = nullptr;
     // The preconditioned modes' B assembly on the tensor cores: tc_prod BF16
     // products per transform (0: the FP64 transforms); tc_on while an assembly
-    // runs its solves there; multipliers [ky][kx] of level 1: Laplacian inverse
-    // and implicit diffusion (tc_mult[0], tc_mult[1]), any mode and level for
+    // runs its solves there; multipliers of level 1: Laplacian inverse and
+    // implicit diffusion (tc_mult[0], tc_mult[1]), any mode and level for
     // ibpm_diag_solve (tc_mult[2])
     int tc_prod = 0;
     bool tc_on = false;
@@ -742,7 +745,7 @@ struct Engine final : ibpm_handle {
                   TcKeep keep = TcKeep{TC_KEEP_ALL, nullptr, {0, 0, 0, 0}}) {
         if (!tc || tc_fmax(tc) < nf) throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms not prepared"};
         const int pe = prof_begin();
-        tc_lines_kernel<In><<<dim3(1, nx, nf), nx / 8, 0, st>>>(in, nx, tc_in_hi(tc), tc_in_lo(tc));
+        tc_lines_kernel<In><<<dim3(1, nx, nf), nx / 8, nx * sizeof(double), st>>>(in, nx, tc_in_hi(tc), tc_in_lo(tc));
         check_launch();
         launches += tc_solve_tail(tc, nf, mtab, out, bs, nx - 1, keep, err + 4, st);
         CK(cudaGetLastError());
@@ -794,7 +797,8 @@ struct Engine final : ibpm_handle {
                     if (lev == L)
                         tc_solve(in_plain(Gl, bs), nbatch, tc_mult[0], Pl, bs, keep);
                     else
-                        tc_solve(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, nbatch, tc_mult[0], Pl, bs, keep);
+                        tc_solve(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, nbatch, tc_mult[0], Pl, bs,
+                                 keep);
                     solved = true;
                 }
             }
@@ -1188,6 +1192,7 @@ void Engine<T>::build_Binv() {
 template <class T>
 void Engine<T>::assemble_invert_B() {
     const int n = 2 * np;
+    const bool rebuilding = uses_binv_start();
     // the preconditioned modes may assemble with the tensor-core transforms
     tc_on = tc_prod > 0 && preconditioned() && tc != nullptr;
     try {
@@ -1202,12 +1207,18 @@ void Engine<T>::assemble_invert_B() {
         throw;
     }
     tc_on = false;
-    // n = 2 np is even: n / 2 two-step launches; after an odd count the result is in Bwork
+    // n = 2 np is even: n / 2 two-step launches, or for the moving-body rebuilds
+    // (rebuilding) eight steps per launch as one block pivot; after an odd count
+    // of launches the result is in Bwork
     int m = 0;
-    for (int k = 0; k < n; k += 2, ++m) {
+    const int step = rebuilding ? 8 : 2;
+    for (int k = 0; k < n; k += step, ++m) {
         const double *src = (m & 1) ? Bwork : Binv;
         double *dst = (m & 1) ? Binv : Bwork;
-        gj_step2_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(src, dst, n, k, err + 1);
+        if (rebuilding)
+            gj_block_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(src, dst, n, k, std::min(step, n - k), err + 1);
+        else
+            gj_step2_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(src, dst, n, k, err + 1);
         check_launch();
     }
     if (m & 1) CK(cudaMemcpyAsync(Binv, Bwork, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, st));
@@ -2004,8 +2015,8 @@ void Engine<T>::set_rebuild_transform(int products) {
         if (!std::is_same<T, double>::value)
             throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms serve the FP64 engine"};
         if (static_bodies) throw ApiError{IBPM_ERR_INVALID, "the B rebuild exists for moving bodies only"};
-        if (nx != ny || (nx != 256 && nx != 512 && nx != 1024))
-            throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms need nx = ny in {256, 512, 1024}"};
+        if (nx != ny || (nx != 256 && nx != 512))
+            throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms need nx = ny in {256, 512}"};
         tc_prepare(kbatch, products);
     }
     if (products != tc_prod) {
@@ -2256,10 +2267,10 @@ void Engine<T>::diag_solve(int op, int level, const double *b, double *x) {
     if (op >= 3) {
         if constexpr (std::is_same<T, double>::value) {
             tc_prepare(1, op < 6 ? 1 : 3);
-            if (!tc_mult[2]) tc_mult[2] = dalloc<float>((size_t)nx * nx);
-            tc_mult_table(mode, level, tc_mult[2]);
             double *bd = staging((size_t)ng);
             CK(cudaMemcpyAsync(bd, b, sizeof(double) * ng, cudaMemcpyHostToDevice, st));
+            if (!tc_mult[2]) tc_mult[2] = dalloc<float>((size_t)nx * nx);
+            tc_mult_table(mode, level, tc_mult[2]);
             tc_solve(InPlain<double>{bd, ng, nx - 1}, 1, tc_mult[2], rhs, ng);
             CK(cudaMemcpyAsync(x, rhs, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(err_h + 4, err + 4, sizeof(int), cudaMemcpyDeviceToHost, st));

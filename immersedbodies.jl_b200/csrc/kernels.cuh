@@ -933,6 +933,74 @@ static __global__ void gj_step2_kernel(const double *__restrict__ S, double *__r
     D[i + (long long)n * j] = v;
 }
 
+// Steps k .. k + b - 1 (b <= 8) of the same elimination in one launch, as one
+// block pivot: with K = {k .. k + b - 1}, P = S_KK^-1 (formed here by b
+// unpivoted steps on the b x b block),
+//   D_KK = P, D_KR = P S_KR, D_RK = -S_RK P, D_RR = S_RR - S_RK P S_KR,
+// which equals the b single steps in exact arithmetic (not bit for bit).  One
+// block per column j, threads over rows i (n <= blockDim.x * gridDim.x).  A
+// pivot <= 0 sets *err to its step + 1.
+static __global__ void gj_block_kernel(const double *__restrict__ S, double *__restrict__ D, int n, int k, int b,
+                                       int *err) {
+    __shared__ double Pm[8][8];
+    __shared__ double T[8];  // P S_Kj for this block's column j
+    const int j = blockIdx.y, t = threadIdx.x;
+    if (t < 64) {
+        const int a = t / 8, c = t % 8;
+        Pm[a][c] = (a < b && c < b) ? S[(k + a) + (long long)n * (k + c)] : 0.0;
+    }
+    __syncthreads();
+    // in-place unpivoted Gauss-Jordan of the b x b block, thread t < 64 owning (t / 8, t % 8)
+    const int a = t / 8, c = t % 8;
+    for (int q = 0; q < b; ++q) {
+        double p = 0.0, aq = 0.0, qc = 0.0, ac = 0.0;
+        if (t < 64) {
+            p = Pm[q][q];
+            aq = Pm[a][q];
+            qc = Pm[q][c];
+            ac = Pm[a][c];
+        }
+        __syncthreads();
+        if (t == 0 && blockIdx.x == 0 && j == 0 && !(p > 0.0)) atomicCAS(err, 0, k + q + 1);
+        if (t < 64 && a < b && c < b) {
+            const double ip = 1.0 / p;
+            if (a == q && c == q)
+                Pm[a][c] = ip;
+            else if (a == q)
+                Pm[a][c] = qc * ip;
+            else if (c == q)
+                Pm[a][c] = -aq * ip;
+            else
+                Pm[a][c] = ac - aq * (qc * ip);
+        }
+        __syncthreads();
+    }
+    const bool jk = j >= k && j < k + b;
+    if (t < b) {
+        double v = 0.0;
+        if (!jk)
+            for (int e = 0; e < b; ++e) v += Pm[t][e] * S[(k + e) + (long long)n * j];
+        T[t] = v;
+    }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + t;
+    if (i >= n) return;
+    const bool ik = i >= k && i < k + b;
+    double v;
+    if (ik && jk) {
+        v = Pm[i - k][j - k];
+    } else if (ik) {
+        v = T[i - k];
+    } else if (jk) {
+        v = 0.0;
+        for (int e = 0; e < b; ++e) v -= S[i + (long long)n * (k + e)] * Pm[e][j - k];
+    } else {
+        v = S[i + (long long)n * j];
+        for (int e = 0; e < b; ++e) v -= S[i + (long long)n * (k + e)] * T[e];
+    }
+    D[i + (long long)n * j] = v;
+}
+
 // Identity columns [c0, c0+nb) of a 2np-length basis, one per batch.
 static __global__ void unit_columns_kernel(double *__restrict__ f, int n, int c0, int nb) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,11 +1,20 @@
 // Dense DST-I passes on the fifth-generation tensor cores (see tc_dst.h).
 //
-// A tile is D[k][l] for 128 output frequencies k (rows of S) and 256 lines l of
-// one field over the whole line length P, accumulated in 256 columns of tensor
-// memory by tcgen05.mma (M 128, N 256, K 16; BF16 x BF16 -> FP32) from K-blocks
-// of 64 elements (128-byte rows, 128-byte swizzle) that TMA brings into a ring
-// of shared-memory stages; the epilogue reads its rows with tcgen05.ld and
-// writes row k as line k of the next pass (rows become lines).
+// A tile is D[r][l] for 128 output frequencies r (rows of the half-length
+// matrix A, block order) and the TN = P/2 lines l of one block of one field
+// (the odd or the even physical indices), over the P/2 slots of the u half (odd
+// frequencies) or the v half (even ones).  It accumulates in TN columns of
+// tensor memory by tcgen05.mma (M 128, N TN, K 16; BF16 x BF16 -> FP32) from
+// K-blocks of 64 elements (128-byte rows, 128-byte swizzle) that TMA brings into
+// a ring of shared-memory stages.  One CTA per SM walks the tiles (M-tiles
+// fastest, so the CTAs working at once share each line tile through L2); two
+// accumulators let the epilogue of one tile run while the products of the next
+// accumulate.  Warps: 0 producer (one lane), 1 products (one lane; the whole
+// warp allocates and frees the tensor memory), 2..5 epilogue (warp w reads lanes
+// 32 (w % 4) ..).  The epilogue turns row r into line r of the next pass: the
+// tile's lines are mirror pairs c, TN - 1 - c (physical j, P - j), so a row's u
+// and v values for the next pass are sums and differences of its own columns.
+//
 // Every wait on an mbarrier gives up after one second of global time, sets the
 // caller's error flag and lets the CTA finish (freeing its tensor memory); no wait
 // depends on another CTA.  No load here uses cluster-wide delivery.
@@ -20,28 +29,37 @@
 
 namespace {
 
-constexpr int kTileM = 128;   // rows of S per CTA
-constexpr int kTileN = 256;   // lines per CTA
+constexpr int kTileM = 128;   // rows of A per tile
 constexpr int kBlockK = 64;   // elements per K-block: one 128-byte swizzle row
-constexpr uint32_t kTmemCols = 256;
 constexpr int kBytesA = kTileM * kBlockK * 2;  // 16 KB
-constexpr int kBytesB = kTileN * kBlockK * 2;  // 32 KB
+constexpr int kThreads = 192;
+constexpr int kStageLd = 33;
+constexpr int kStageFloats = 32 * kStageLd;
 
-enum { EPI_SPLIT = 0, EPI_MULT = 1, EPI_F64 = 2 };
+// EPI_SPLIT_NAT: as EPI_SPLIT, with the next pass's lines in natural order
+// (line x - 1 for frequency x, the padding last), so that the last pass's
+// columns are contiguous physical positions
+enum { EPI_SPLIT = 0, EPI_MULT = 1, EPI_F64 = 2, EPI_SPLIT_NAT = 3 };
 
-template <int NPROD>
+template <int NPROD, int P>
 struct Cfg {
+    static constexpr int kTN = P / 2;                      // lines per tile, the MMA's N
+    static constexpr int kBytesB = kTN * kBlockK * 2;
     static constexpr int kParts = NPROD == 3 ? 2 : 1;
     static constexpr int kStageBytes = kParts * (kBytesA + kBytesB);
-    static constexpr int kStages = NPROD == 3 ? 2 : 4;
+    static constexpr int kStages = (192 * 1024) / kStageBytes > 6 ? 6 : (192 * 1024) / kStageBytes;
+    static constexpr uint32_t kTmemCols = 2 * kTN;        // two accumulators
+    static constexpr int kKB = (P / 2) / kBlockK;          // K-blocks per tile
     // the operand ring, four epilogue staging tiles and alignment slack
-    static constexpr size_t kSmem = (size_t)kStages * kStageBytes + 4 * 32 * 33 * sizeof(float) + 1024;
+    static constexpr size_t kSmem = (size_t)kStages * kStageBytes + 4 * kStageFloats * sizeof(float) + 1024;
+    // kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M 128, N kTN
+    static constexpr uint32_t kIdesc =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTN >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
 };
 
 struct PassArgs {
-    int P;
     __nv_bfloat16 *oh, *ol;   // next pass's lines (EPI_SPLIT, EPI_MULT)
-    const float *mult;        // [k][l] multipliers (EPI_MULT)
+    const float *mult;        // [l][r] multipliers (EPI_MULT)
     double *out;              // result (EPI_F64)
     long long bs;
     int ld;
@@ -49,13 +67,16 @@ struct PassArgs {
     int *err;
 };
 
-// 0-based (x, y) of the result: stored or not
-__device__ __forceinline__ bool kept(const TcKeep &k, int x, int y) {
+// The result selection as bounds on 0-based physical (x, y): stored when
+// (x in [x0, x1] and y in [y0, y1]) or y in {ya, yb} or x in {xa, xb}
+struct Keep {
+    int x0, x1, y0, y1, ya, yb, xa, xb;
+};
+__device__ __forceinline__ Keep keep_bounds(const TcKeep &k) {
     if (k.mode == TC_KEEP_WINDOW)
-        return x >= k.win[0] - 2 && x <= k.win[1] && y >= k.win[2] - 2 && y <= k.win[3];
-    if (k.mode == TC_KEEP_LINES)
-        return y == k.lines[0] || y == k.lines[1] || x == k.lines[2] || x == k.lines[3];
-    return true;
+        return Keep{__ldg(k.win) - 2, __ldg(k.win + 1), __ldg(k.win + 2) - 2, __ldg(k.win + 3), -1, -1, -1, -1};
+    if (k.mode == TC_KEEP_LINES) return Keep{0, -1, 0, -1, k.lines[0], k.lines[1], k.lines[2], k.lines[3]};
+    return Keep{0, 1 << 30, 0, 1 << 30, -1, -1, -1, -1};
 }
 
 __device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -118,16 +139,12 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t a) {
     return d;
 }
 
-// kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M 128, N 256
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTileN >> 3) << 17) |
-                            ((uint32_t)(kTileM >> 4) << 24);
-
-__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
         : "memory");
 }
 
@@ -149,86 +166,124 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Rows row0 .. row0 + 31 of a tile (one warp, lane = row), columns col0 .. col0
-// + 31 (v: FP32 bits from tensor memory): multiplied (EPI_MULT), then stored as
-// the next pass's BF16 parts (EPI_SPLIT, EPI_MULT) or as the FP64 result
-// (EPI_F64: interior elements that the selection keeps).  The warp's staging
-// tile stg (32 x 33 floats, conflict-free both ways) turns the stores into
-// coalesced 64-byte (BF16) and 256-byte (FP64) row segments.
-constexpr int kStageLd = 33;
-constexpr int kStageFloats = 32 * kStageLd;
 
-template <int NPROD, int EPI>
-__device__ __forceinline__ void epilogue_staged(const PassArgs &a, int f, int row0, int col0, const uint32_t (&v)[32],
-                                                float *stg) {
-    const int lane = threadIdx.x & 31, P = a.P;
-    float x[32];
+// Rows row0 .. row0 + 31 (one warp, lane = row) of a 32 x 32 block staged in
+// stg (32 x 33 floats, conflict-free both ways) to the next pass's lines at
+// slots pos0 .. pos0 + 31, as BF16 parts in coalesced 64-byte row segments;
+// row r becomes line r, or (NAT) the natural-order line of its frequency.
+template <int NPROD, int P, bool NAT>
+__device__ __forceinline__ void store_staged(const PassArgs &a, int f, int row0, int pos0, const float *stg) {
+    const int lane = threadIdx.x & 31, q = lane & 3;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) x[j] = __uint_as_float(v[j]);
-    if (EPI == EPI_MULT) {
-        const float4 *mp = reinterpret_cast<const float4 *>(a.mult + (size_t)(row0 + lane) * P + col0);
+    for (int it = 0; it < 4; ++it) {
+        const int r = it * 8 + (lane >> 2);
+        __align__(16) __nv_bfloat16 h[8];
+        __align__(16) __nv_bfloat16 l[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const float4 m = __ldg(mp + q);
-            x[4 * q] *= m.x;
-            x[4 * q + 1] *= m.y;
-            x[4 * q + 2] *= m.z;
-            x[4 * q + 3] *= m.w;
+        for (int i = 0; i < 8; ++i) tc_split(stg[r * kStageLd + 8 * q + i], h[i], l[i]);
+        int line = row0 + r;
+        if (NAT) {
+            const int k = tc_blk(line, P);
+            line = k == 0 ? P - 1 : k - 1;
         }
+        const size_t off = ((size_t)f * P + line) * P + pos0 + 8 * q;
+        *reinterpret_cast<uint4 *>(a.oh + off) = *reinterpret_cast<const uint4 *>(h);
+        if (NPROD == 3) *reinterpret_cast<uint4 *>(a.ol + off) = *reinterpret_cast<const uint4 *>(l);
     }
-#pragma unroll
-    for (int j = 0; j < 32; ++j) stg[lane * kStageLd + j] = x[j];
-    __syncwarp();
-    if (EPI == EPI_F64) {
-        const int col = col0 + lane;
-        double *o = a.out + (long long)f * a.bs + col;
-        for (int r = 0; r < 32; ++r) {
-            const int row = row0 + r;
-            if (row < P - 1 && col < P - 1 && kept(a.keep, col, row))
-                o[(long long)row * a.ld] = (double)stg[r * kStageLd + lane];
-        }
-    } else {
-        const int q = lane & 3;
-#pragma unroll
-        for (int it = 0; it < 4; ++it) {
-            const int r = it * 8 + (lane >> 2);
-            __align__(16) __nv_bfloat16 h[8];
-            __align__(16) __nv_bfloat16 l[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) tc_split(stg[r * kStageLd + 8 * q + i], h[i], l[i]);
-            const size_t off = ((size_t)f * P + row0 + r) * P + col0 + 8 * q;
-            *reinterpret_cast<uint4 *>(a.oh + off) = *reinterpret_cast<const uint4 *>(h);
-            if (NPROD == 3) *reinterpret_cast<uint4 *>(a.ol + off) = *reinterpret_cast<const uint4 *>(l);
-        }
-    }
-    __syncwarp();
 }
 
-// One CTA per SM walks the tiles (M-tiles fastest, so the CTAs working at once
-// share each line tile through L2).  Two accumulators of
-// 256 tensor-memory columns let the epilogue of one tile run while the products
-// of the next accumulate.  Warps: 0 producer (one lane), 1 products (one lane;
-// the whole warp allocates and frees the 512 columns), 2..5 epilogue (warp w
-// reads lanes 32 (w % 4) ..).
-constexpr int kThreads = 192;
+// The epilogue of one tile for one warp: rows row0 + lane of accumulator acc
+// (this warp's lane quarter, the buffer's first column), lines of block nt.
+template <int NPROD, int EPI, int P>
+__device__ __forceinline__ void epilogue(const PassArgs &a, int f, int row0, int nt, uint32_t acc, float *stg) {
+    using C = Cfg<NPROD, P>;
+    constexpr int TN = C::kTN, NCH = TN / 32;
+    const int lane = threadIdx.x & 31, row = row0 + lane;
+    if constexpr (EPI == EPI_F64) {
+        // row flags of the warp's 32 rows (bit rr: row row0 + rr), column flags per lane
+        const Keep kb = keep_bounds(a.keep);
+        const int y = tc_blk(row, P) - 1;  // this thread's physical row (-1: padding)
+        const unsigned live = __ballot_sync(0xffffffffu, y >= 0);
+        const unsigned in_rows = __ballot_sync(0xffffffffu, y >= 0 && y >= kb.y0 && y <= kb.y1);
+        const unsigned on_rows = __ballot_sync(0xffffffffu, y >= 0 && (y == kb.ya || y == kb.yb));
+        double *o = a.out + (long long)f * a.bs;
+        for (int k = 0; k < NCH; ++k) {
+            // this lane's physical column: the lines arrive in natural order
+            const int x = nt * TN + 32 * k + lane < P - 1 ? nt * TN + 32 * k + lane : -1;
+            const bool cin = x >= 0 && x >= kb.x0 && x <= kb.x1, con = x >= 0 && (x == kb.xa || x == kb.xb);
+            // rows with anything to store in this chunk
+            const unsigned rows =
+                (__any_sync(0xffffffffu, cin) ? in_rows : 0u) | on_rows | (__any_sync(0xffffffffu, con) ? live : 0u);
+            if (rows == 0u) continue;
+            uint32_t v[32];
+            tmem_ld32(acc + (uint32_t)(32 * k), v);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) stg[lane * kStageLd + i] = __uint_as_float(v[i]);
+            __syncwarp();
+            const unsigned mine = (cin ? in_rows : 0u) | on_rows | (con ? live : 0u);  // rows this lane stores
+            for (unsigned rest = rows; rest;) {
+                const int rr = __ffs(rest) - 1;
+                rest &= rest - 1;
+                const int yy = __shfl_sync(0xffffffffu, y, rr);
+                if (x >= 0 && ((mine >> rr) & 1u)) o[x + a.ld * yy] = (double)stg[rr * kStageLd + lane];
+            }
+            __syncwarp();
+        }
+    } else {
+        for (int k = 0; k < NCH / 2; ++k) {
+            uint32_t va[32], vb[32];
+            tmem_ld32(acc + (uint32_t)(32 * k), va);
+            tmem_ld32(acc + (uint32_t)(32 * (NCH - 1 - k)), vb);
+            float x[32], y[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                x[i] = __uint_as_float(va[i]);
+                y[i] = __uint_as_float(vb[i]);
+            }
+            if (EPI == EPI_MULT) {
+                // column l of the table holds the rows' multipliers contiguously
+                const float *ma = a.mult + (size_t)(nt * TN + 32 * k) * P + row;
+                const float *mb = a.mult + (size_t)(nt * TN + 32 * (NCH - 1 - k)) * P + row;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    x[i] *= __ldg(ma + (size_t)i * P);
+                    y[i] *= __ldg(mb + (size_t)i * P);
+                }
+            }
+            // column 32k + i pairs with TN - 1 - (32k + i) = 32 (NCH - 1 - k) + 31 - i
+            const int slot = nt * (TN / 2) + 32 * k;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) stg[lane * kStageLd + i] = x[i] + y[31 - i];
+            __syncwarp();
+            store_staged<NPROD, P, EPI == EPI_SPLIT_NAT>(a, f, row0, slot, stg);
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 32; ++i) stg[lane * kStageLd + i] = x[i] - y[31 - i];
+            __syncwarp();
+            store_staged<NPROD, P, EPI == EPI_SPLIT_NAT>(a, f, row0, P / 2 + slot, stg);
+            __syncwarp();
+        }
+    }
+}
 
-template <int NPROD, int EPI>
+template <int NPROD, int EPI, int P>
 __global__ void __launch_bounds__(kThreads, 1)
-    tc_dst_pass_kernel(const __grid_constant__ CUtensorMap tSh, const __grid_constant__ CUtensorMap tSl,
-                             const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl,
-                             PassArgs a, int nf) {
-    using C = Cfg<NPROD>;
+    tc_dst_pass_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
+                       const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl, PassArgs a,
+                       int nf) {
+    using C = Cfg<NPROD, P>;
+    constexpr int TN = C::kTN, MT = P / kTileM, NT = 2, KB = C::kKB;
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t full[C::kStages], empty[C::kStages], accf[2], acce[2], fin;
     __shared__ uint32_t tmem_s;
     __shared__ int fail_s;
+    // the 128-byte swizzle atoms must start on 1024-byte boundaries of the shared window
     uint8_t *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int P = a.P, KB = P / kBlockK, MT = P / kTileM, NT = P / kTileN;
+    const int ntiles = nf * MT * NT;
     // epilogue warp w (2..5) stages through its own tile after the operand ring
     float *stg = reinterpret_cast<float *>(smem + (size_t)C::kStages * C::kStageBytes) +
                  (warp >= 2 ? (warp - 2) * kStageFloats : 0);
-    const int ntiles = nf * MT * NT;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::kStages; ++s) {
@@ -246,7 +301,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&tmem_s)),
-                     "r"(2 * kTmemCols)
+                     "r"(C::kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -257,14 +312,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     auto stage_a = [&](int s, int part) { return smem + (size_t)s * C::kStageBytes + part * kBytesA; };
     auto stage_b = [&](int s, int part) {
-        return smem + (size_t)s * C::kStageBytes + C::kParts * kBytesA + part * kBytesB;
+        return smem + (size_t)s * C::kStageBytes + C::kParts * kBytesA + part * C::kBytesB;
     };
 
     if (warp == 0) {
         if (lane == 0) {
             int kc = 0;  // K-blocks loaded so far (the ring position)
             for (int t = blockIdx.x; t < ntiles && !fail_s; t += gridDim.x) {
-                const int m0 = (t % MT) * kTileM, n0 = ((t / MT) % NT) * kTileN, f = t / (MT * NT);
+                const int m0 = (t % MT) * kTileM, n0 = ((t / MT) % NT) * TN, f = t / (MT * NT);
+                const int koff = m0 < P / 2 ? 0 : P / 2;  // odd frequencies read u, even ones v
                 for (int kb = 0; kb < KB; ++kb, ++kc) {
                     const int s = kc % C::kStages;
                     if (kc >= C::kStages && !mbar_wait(&empty[s], ((kc / C::kStages) - 1) & 1)) {
@@ -272,12 +328,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     mbar_expect_tx(&full[s], C::kStageBytes);
-                    const int x = kb * kBlockK;
-                    tma_load(stage_a(s, 0), &tSh, &full[s], x, m0);
-                    tma_load(stage_b(s, 0), &tXh, &full[s], x, f * P + n0);
+                    tma_load(stage_a(s, 0), &tAh, &full[s], kb * kBlockK, m0);
+                    tma_load(stage_b(s, 0), &tXh, &full[s], koff + kb * kBlockK, f * P + n0);
                     if (NPROD == 3) {
-                        tma_load(stage_a(s, 1), &tSl, &full[s], x, m0);
-                        tma_load(stage_b(s, 1), &tXl, &full[s], x, f * P + n0);
+                        tma_load(stage_a(s, 1), &tAl, &full[s], kb * kBlockK, m0);
+                        tma_load(stage_b(s, 1), &tXl, &full[s], koff + kb * kBlockK, f * P + n0);
                     }
                 }
             }
@@ -292,7 +347,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                const uint32_t acc = tmem + (uint32_t)(b * kTmemCols);
+                const uint32_t acc = tmem + (uint32_t)(b * TN);
                 bool ok = true;
                 for (int kb = 0; kb < KB; ++kb, ++kc) {
                     const int s = kc % C::kStages;
@@ -306,11 +361,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint64_t bl = sw128_desc(saddr(stage_b(s, NPROD == 3 ? 1 : 0)));
 #pragma unroll
                     for (int kk = 0; kk < kBlockK / 16; ++kk) {
-                        const uint64_t o = (uint64_t)(kk * 32 >> 4);
-                        mma(acc, ah + o, bh + o, (kb | kk) != 0);
+                        const uint64_t o = (uint64_t)(kk * 32 >> 4);  // 16 elements = 32 B along the swizzled row
+                        mma(acc, ah + o, bh + o, C::kIdesc, (kb | kk) != 0);
                         if (NPROD == 3) {
-                            mma(acc, ah + o, bl + o, 1);
-                            mma(acc, al + o, bh + o, 1);
+                            mma(acc, ah + o, bl + o, C::kIdesc, 1);
+                            mma(acc, al + o, bh + o, C::kIdesc, 1);
                         }
                     }
                     mma_commit(&empty[s]);
@@ -337,13 +392,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 atomicExch(&fail_s, 1);
                 break;
             }
-            const int m0 = (t % MT) * kTileM, n0 = ((t / MT) % NT) * kTileN, f = t / (MT * NT);
-            const uint32_t acc = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTmemCols);
-            for (int c = 0; c < kTileN; c += 32) {
-                uint32_t v[32];
-                tmem_ld32(acc + (uint32_t)c, v);
-                epilogue_staged<NPROD, EPI>(a, f, m0 + q * 32, n0 + c, v, stg);
-            }
+            const int m0 = (t % MT) * kTileM, nt = (t / MT) % NT, f = t / (MT * NT);
+            const uint32_t acc = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN);
+            epilogue<NPROD, EPI, P>(a, f, m0 + q * 32, nt, acc, stg);
             tc_fence_before();
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(&acce[b])) : "memory");
         }
@@ -354,7 +405,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (fail_s && threadIdx.x == 0) atomicExch(a.err, 1);
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTmemCols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::kTmemCols)
                      : "memory");
     }
 }
@@ -378,12 +429,12 @@ EncodeTiled encoder() {
     return fn;
 }
 
-// 2D BF16 map over rows x P (row-major), boxes of box_rows x 64 elements, 128-byte swizzle
-bool make_map(CUtensorMap *m, void *base, int P, long long rows, int box_rows) {
+// 2D BF16 map over rows x cols (row-major), boxes of box_rows x 64 elements, 128-byte swizzle
+bool make_map(CUtensorMap *m, void *base, int cols, long long rows, int box_rows) {
     EncodeTiled enc = encoder();
     if (!enc) return false;
-    const cuuint64_t dims[2] = {(cuuint64_t)P, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)P * 2};
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
     const cuuint32_t box[2] = {(cuuint32_t)kBlockK, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -405,25 +456,32 @@ float bf16_value(uint16_t b) {
     return v;
 }
 
-template <int NPROD, int EPI>
-bool set_smem_attr() {
-    return cudaFuncSetAttribute(tc_dst_pass_kernel<NPROD, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)Cfg<NPROD>::kSmem) == cudaSuccess;
+template <int NPROD, int P>
+bool set_smem_attrs() {
+    const int sm = (int)Cfg<NPROD, P>::kSmem;
+    return cudaFuncSetAttribute(tc_dst_pass_kernel<NPROD, EPI_SPLIT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                sm) == cudaSuccess &&
+           cudaFuncSetAttribute(tc_dst_pass_kernel<NPROD, EPI_MULT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                sm) == cudaSuccess &&
+           cudaFuncSetAttribute(tc_dst_pass_kernel<NPROD, EPI_F64, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                sm) == cudaSuccess &&
+           cudaFuncSetAttribute(tc_dst_pass_kernel<NPROD, EPI_SPLIT_NAT, P>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, sm) == cudaSuccess;
 }
 
 }  // namespace
 
 struct TcDstPlan {
     int P = 0, fmax = 0, nprod = 1, nsm = 148;
-    __nv_bfloat16 *S[2] = {nullptr, nullptr};
+    __nv_bfloat16 *A[2] = {nullptr, nullptr};                            // hi, lo: P x P/2
     __nv_bfloat16 *X[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [buffer][hi, lo]
-    CUtensorMap mS[2], mX[2][2];
+    CUtensorMap mA[2], mX[2][2];
 };
 
 static void tc_free(TcDstPlan *p) {
     if (!p) return;
-    cudaFree(p->S[0]);
-    cudaFree(p->S[1]);
+    cudaFree(p->A[0]);
+    cudaFree(p->A[1]);
     for (auto &b : p->X)
         for (auto *q : b) cudaFree(q);
     delete p;
@@ -435,7 +493,7 @@ TcDstPlan *tc_create(int P, int fmax, int nprod, const char **why) {
         tc_free(p);
         return nullptr;
     };
-    if (P != 256 && P != 512 && P != 1024) return fail(nullptr, "tensor-core transforms need nx = ny in {256, 512, 1024}");
+    if (P != 256 && P != 512) return fail(nullptr, "tensor-core transforms need nx = ny in {256, 512}");
     if (nprod != 1 && nprod != 3) return fail(nullptr, "tensor-core transforms take 1 or 3 products");
     if (fmax < 1 || (long long)fmax * P > (1LL << 31)) return fail(nullptr, "bad field count");
     int dev = 0;
@@ -449,40 +507,48 @@ TcDstPlan *tc_create(int P, int fmax, int nprod, const char **why) {
     p->P = P;
     p->fmax = fmax;
     p->nprod = nprod;
-    const size_t nS = (size_t)P * P, nX = (size_t)fmax * P * P;
+    const int H = P / 2;
+    const size_t nA = (size_t)P * H, nX = (size_t)fmax * P * P;
     const int parts = nprod == 3 ? 2 : 1;
     for (int k = 0; k < parts; ++k)
-        if (cudaMalloc(&p->S[k], nS * 2) != cudaSuccess) return fail(p, "out of device memory");
+        if (cudaMalloc(&p->A[k], nA * 2) != cudaSuccess) return fail(p, "out of device memory");
     for (int b = 0; b < 2; ++b)
         for (int k = 0; k < parts; ++k)
             if (cudaMalloc(&p->X[b][k], nX * 2) != cudaSuccess) return fail(p, "out of device memory");
-    // S[k][j] = 2 sin(pi (k+1)(j+1) / P) on the (P-1)^2 block, zero in the padding row and column
-    std::vector<uint16_t> hi(nS, 0), lo(nS, 0);
-    for (int k = 0; k < P - 1; ++k)
-        for (int j = 0; j < P - 1; ++j) {
-            const long long t = ((long long)(k + 1) * (j + 1)) % (2LL * P);
-            const double s = 2.0 * std::sin(M_PI * (double)t / (double)P);
-            const uint16_t h = bf16_bits((float)s);
-            hi[(size_t)k * P + j] = h;
-            lo[(size_t)k * P + j] = bf16_bits((float)(s - (double)bf16_value(h)));
+    // A[r][s] = 2 sin(pi k j / P), k = tc_blk(r) (the frequency of row r) and j =
+    // tc_uvj(s) (the pair of slot s); zero for the padding row and for even k at
+    // j = P/2, whose v slot holds no pair
+    std::vector<uint16_t> hi(nA, 0), lo(nA, 0);
+    for (int r = 0; r < P; ++r) {
+        const int k = tc_blk(r, P);
+        if (k == 0) continue;
+        for (int s = 0; s < H; ++s) {
+            const int j = tc_uvj(s, P);
+            if (k % 2 == 0 && j == H) continue;
+            const long long t = ((long long)k * j) % (2LL * P);
+            const double v = 2.0 * std::sin(M_PI * (double)t / (double)P);
+            const uint16_t h = bf16_bits((float)v);
+            hi[(size_t)r * H + s] = h;
+            lo[(size_t)r * H + s] = bf16_bits((float)(v - (double)bf16_value(h)));
         }
-    if (cudaMemcpy(p->S[0], hi.data(), nS * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
-        (parts == 2 && cudaMemcpy(p->S[1], lo.data(), nS * 2, cudaMemcpyHostToDevice) != cudaSuccess))
+    }
+    if (cudaMemcpy(p->A[0], hi.data(), nA * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
+        (parts == 2 && cudaMemcpy(p->A[1], lo.data(), nA * 2, cudaMemcpyHostToDevice) != cudaSuccess))
         return fail(p, "copy of the transform matrix failed");
     for (int k = 0; k < parts; ++k)
-        if (!make_map(&p->mS[k], p->S[k], P, P, kTileM)) return fail(p, "tensor map encoding failed");
+        if (!make_map(&p->mA[k], p->A[k], H, P, kTileM)) return fail(p, "tensor map encoding failed");
     for (int b = 0; b < 2; ++b)
         for (int k = 0; k < parts; ++k)
-            if (!make_map(&p->mX[b][k], p->X[b][k], P, (long long)fmax * P, kTileN))
-                return fail(p, "tensor map encoding failed");
+            if (!make_map(&p->mX[b][k], p->X[b][k], P, (long long)fmax * P, H)) return fail(p, "tensor map encoding failed");
     if (parts == 1) {
-        p->mS[1] = p->mS[0];
+        p->mA[1] = p->mA[0];
         for (int b = 0; b < 2; ++b) p->mX[b][1] = p->mX[b][0];
     }
-    const bool attrs = nprod == 3 ? (set_smem_attr<3, EPI_SPLIT>() && set_smem_attr<3, EPI_MULT>() &&
-                                     set_smem_attr<3, EPI_F64>())
-                                  : (set_smem_attr<1, EPI_SPLIT>() && set_smem_attr<1, EPI_MULT>() &&
-                                     set_smem_attr<1, EPI_F64>());
+    bool attrs;
+    if (P == 512)
+        attrs = nprod == 3 ? set_smem_attrs<3, 512>() : set_smem_attrs<1, 512>();
+    else
+        attrs = nprod == 3 ? set_smem_attrs<3, 256>() : set_smem_attrs<1, 256>();
     if (!attrs) return fail(p, "shared-memory attribute refused");
     return p;
 }
@@ -494,25 +560,26 @@ int tc_fmax(const TcDstPlan *p) { return p->fmax; }
 __nv_bfloat16 *tc_in_hi(TcDstPlan *p) { return p->X[0][0]; }
 __nv_bfloat16 *tc_in_lo(TcDstPlan *p) { return p->nprod == 3 ? p->X[0][1] : nullptr; }
 
-template <int NPROD>
+template <int NPROD, int P>
 static void tc_pass(TcDstPlan *p, int src, int epi, int nf, PassArgs a, cudaStream_t st) {
-    const CUtensorMap &sh = p->mS[0], &sl = p->mS[1], &xh = p->mX[src][0], &xl = p->mX[src][1];
-    const int ntiles = nf * (p->P / kTileM) * (p->P / kTileN);
+    const CUtensorMap &ah = p->mA[0], &al = p->mA[1], &xh = p->mX[src][0], &xl = p->mX[src][1];
+    const int ntiles = nf * (P / kTileM) * 2;
     const int g = ntiles < p->nsm ? ntiles : p->nsm;
-    const size_t sm = Cfg<NPROD>::kSmem;
+    const size_t sm = Cfg<NPROD, P>::kSmem;
     if (epi == EPI_SPLIT)
-        tc_dst_pass_kernel<NPROD, EPI_SPLIT><<<g, kThreads, sm, st>>>(sh, sl, xh, xl, a, nf);
+        tc_dst_pass_kernel<NPROD, EPI_SPLIT, P><<<g, kThreads, sm, st>>>(ah, al, xh, xl, a, nf);
     else if (epi == EPI_MULT)
-        tc_dst_pass_kernel<NPROD, EPI_MULT><<<g, kThreads, sm, st>>>(sh, sl, xh, xl, a, nf);
+        tc_dst_pass_kernel<NPROD, EPI_MULT, P><<<g, kThreads, sm, st>>>(ah, al, xh, xl, a, nf);
+    else if (epi == EPI_SPLIT_NAT)
+        tc_dst_pass_kernel<NPROD, EPI_SPLIT_NAT, P><<<g, kThreads, sm, st>>>(ah, al, xh, xl, a, nf);
     else
-        tc_dst_pass_kernel<NPROD, EPI_F64><<<g, kThreads, sm, st>>>(sh, sl, xh, xl, a, nf);
+        tc_dst_pass_kernel<NPROD, EPI_F64, P><<<g, kThreads, sm, st>>>(ah, al, xh, xl, a, nf);
 }
 
 int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long long bs, int ld, TcKeep keep,
                   int *err, cudaStream_t st) {
     if (nf < 1 || nf > p->fmax) return -1;
     PassArgs a{};
-    a.P = p->P;
     a.mult = mult;
     a.out = out;
     a.bs = bs;
@@ -520,15 +587,22 @@ int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long lon
     a.keep = keep;
     a.err = err;
     // (y, x) -> (kx, y) -> (ky, kx) [x m] -> (x, ky) -> (y, x)
-    const int epis[4] = {EPI_SPLIT, EPI_MULT, EPI_SPLIT, EPI_F64};
+    const int epis[4] = {EPI_SPLIT, EPI_MULT, EPI_SPLIT_NAT, EPI_F64};
     for (int k = 0; k < 4; ++k) {
         const int src = k & 1, dst = src ^ 1;
         a.oh = p->X[dst][0];
         a.ol = p->X[dst][1];
-        if (p->nprod == 3)
-            tc_pass<3>(p, src, epis[k], nf, a, st);
-        else
-            tc_pass<1>(p, src, epis[k], nf, a, st);
+        if (p->P == 512) {
+            if (p->nprod == 3)
+                tc_pass<3, 512>(p, src, epis[k], nf, a, st);
+            else
+                tc_pass<1, 512>(p, src, epis[k], nf, a, st);
+        } else {
+            if (p->nprod == 3)
+                tc_pass<3, 256>(p, src, epis[k], nf, a, st);
+            else
+                tc_pass<1, 256>(p, src, epis[k], nf, a, st);
+        }
     }
     return 4;
 }

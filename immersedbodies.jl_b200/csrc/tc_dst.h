@@ -2,16 +2,25 @@
 // accumulation in tensor memory), for the B assembly of the preconditioned
 // moving-body modes, where B^-1 serves as a preconditioner and need not be exact.
 //
-// A solve x = S(m ⊙ S(b)) of one P x P field (P = nx = ny, the (P-1)^2 interior
-// padded by a zero row and column) is four passes of the same dense product
-//     D[f][k][l] = sum_p S[k][p] X[f][l][p]
-// with S[k][p] = 2 sin(pi (k+1)(p+1) / P) (FFTW's RODFT00, the reference's
-// transform at src/fluid.jl:113-115) as the A operand and the batch's lines as
-// the B operand.  Each pass transforms along one axis and writes its result as
-// the next pass's lines: (y, x) -> (kx, y) -> (ky, kx) with the spectral
-// multiplier applied -> (x, ky) -> (y, x) in FP64.  Operands are BF16: one
-// product S_hi X_hi, or the split form S_hi X_hi + S_hi X_lo + S_lo X_hi with
-// v = hi + lo, lo = bf16(v - hi) (about 16 significant bits per operand).
+// A solve x = S(m ⊙ S(b)) of one P x P field (P = nx = ny, the (P-1)^2 interior)
+// is four passes of one dense product per line, y_k = sum_j S[k][j] x_j with
+// S[k][j] = 2 sin(pi k j / P) (FFTW's RODFT00, the reference's transform at
+// src/fluid.jl:113-115).  Since S[k][P-j] = (-1)^(k+1) S[k][j], odd k need only
+// u_j = x_j + x_(P-j) and even k only v_j = x_j - x_(P-j) (j < P/2; u_(P/2) =
+// x_(P/2)): two products of half the length, half the work of the full one.
+//
+// Storage.  A line is held in "uv form": P BF16 values, u in slots [0, P/2) and
+// v in [P/2, P); slot s (s' = s mod P/2) holds the pair (j, P - j) with j =
+// tc_uvj(s').  Lines are held in "block order": storage index l is physical
+// index tc_blk(l) (odd indices first, then the even ones arranged so that l and
+// P/2 - 1 - l, or P - 1 - (l - P/2) in the second half, are mirror pairs j,
+// P - j; one padding slot).  Pass p transforms the lines of its input along
+// their positions: output row r (frequency tc_blk(r)) of the lines of one field
+// becomes line r of pass p + 1, whose positions are pass p's lines:
+//   (y, x) -> (kx, y) -> (ky, kx) [x m] -> (x, ky) -> (y, x) in FP64.
+// Operands are BF16: one product S_hi X_hi, or the split form S_hi X_hi +
+// S_hi X_lo + S_lo X_hi with v = hi + lo, lo = bf16(v - hi) (about 16
+// significant bits per operand).
 #pragma once
 #include <cstdint>
 #include <cuda_bf16.h>
@@ -19,7 +28,20 @@
 
 struct TcDstPlan;
 
-// P in {256, 512, 1024}; fmax fields per call; nprod 1 (BF16) or 3 (split BF16).
+// Physical index (1 .. P-1; 0 for the padding slot) of storage index i in block order.
+__host__ __device__ __forceinline__ int tc_blk(int i, int P) {
+    if (i < P / 2) return 2 * i + 1;
+    const int c = i - P / 2;
+    if (c < P / 4) return 2 * (c + 1);
+    if (c == P / 4) return 0;
+    return 2 * c;
+}
+// Physical index j (1 .. P/2) of the pair (j, P - j) held in uv slot s' (0 .. P/2 - 1).
+__host__ __device__ __forceinline__ int tc_uvj(int s, int P) {
+    return s < P / 4 ? 2 * s + 1 : 2 * (s - P / 4 + 1);
+}
+
+// P in {256, 512}; fmax fields per call; nprod 1 (BF16) or 3 (split BF16).
 // Allocates the transform matrices, two line buffers (hi and lo parts) and the
 // TMA descriptors on the current device.  Returns nullptr (and sets *why) when
 // the device or sizes are unsupported.
@@ -28,7 +50,7 @@ void tc_destroy(TcDstPlan *p);
 int tc_P(const TcDstPlan *p);
 int tc_nprod(const TcDstPlan *p);
 int tc_fmax(const TcDstPlan *p);
-// the buffer the first pass reads: [f][line y][position x], P x P per field
+// the buffer the first pass reads: lines y (block order) of positions x (uv form)
 __nv_bfloat16 *tc_in_hi(TcDstPlan *p);
 __nv_bfloat16 *tc_in_lo(TcDstPlan *p);
 // Which elements of the result a solve stores: all; those a windowed curl
@@ -43,11 +65,12 @@ struct TcKeep {
 };
 
 // Runs the four passes over nf fields whose lines the caller wrote to
-// tc_in_hi / tc_in_lo; mult (device, P x P floats, [ky][kx]) is applied after
-// the second pass; the result goes to out[f * bs + x + ld * y] for x, y < P - 1
-// that `keep` selects.  *err (device) is set to 1 if a wait inside a pass gave
-// up (after one second; never in normal use).  Returns the number of kernels
-// launched.
+// tc_in_hi / tc_in_lo; mult (device, P x P floats, [kx storage][ky storage],
+// both in block order: read coalesced by the rows ky of a tile) is applied
+// after the second pass; the result goes to out[f * bs + x + ld * y] for the x,
+// y < P - 1 that `keep` selects.  *err (device) is set to 1 if a wait inside a
+// pass gave up (after one second; never in normal use).  Returns the number of
+// kernels launched.
 int tc_solve_tail(TcDstPlan *p, int nf, const float *mult, double *out, long long bs, int ld, TcKeep keep,
                   int *err, cudaStream_t st);
 
@@ -58,22 +81,26 @@ __device__ __forceinline__ void tc_split(float v, __nv_bfloat16 &hi, __nv_bfloat
 }
 
 // The first pass's lines from a solve prologue `in` (in(f, i, j): the value at
-// x = i - 1, y = j - 1 of field f, 1 <= i, j <= P - 1): line y of field f holds
-// positions x = 0 .. P - 1, zero in the padding.  Block: P / 8 threads, 8
-// positions each; grid (1, P, nf).
+// 1-based (i, j) of field f, 1 <= i, j <= P - 1): line l of field f is physical
+// row y = tc_blk(l) in uv form (zero for the padding line).  The row is read
+// once, coalesced, into shared memory (P doubles); thread t then forms slots t,
+// t + P/8, ... (neighbouring threads read neighbouring pairs).  Block: P / 8
+// threads; grid (1, P, nf); P * 8 bytes of shared memory.
 template <class In>
 __global__ void tc_lines_kernel(In in, int P, __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
-    const int f = blockIdx.z, y = blockIdx.y, x0 = threadIdx.x * 8;
-    __align__(16) __nv_bfloat16 h[8];
-    __align__(16) __nv_bfloat16 l[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int x = x0 + j;
-        const double v = (x < P - 1 && y < P - 1) ? in(f, x + 1, y + 1) : 0.0;
-        h[j] = __double2bfloat16(v);
-        l[j] = __double2bfloat16(v - (double)__bfloat162float(h[j]));
+    extern __shared__ double tc_row[];
+    const int f = blockIdx.z, l = blockIdx.y, t = threadIdx.x, nt = blockDim.x;
+    const int y = tc_blk(l, P);
+    for (int x = t + 1; x < P; x += nt) tc_row[x] = y != 0 ? in(f, x, y) : 0.0;
+    __syncthreads();
+    const size_t off = ((size_t)f * P + l) * P;
+    for (int s = t; s < P; s += nt) {
+        const int half = s >= P / 2;
+        const int x = tc_uvj(half ? s - P / 2 : s, P);
+        const double a = tc_row[x], b = x == P / 2 ? 0.0 : tc_row[P - x];
+        const double v = half ? (x == P / 2 ? 0.0 : a - b) : a + b;
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        hi[off + s] = h;
+        if (lo) lo[off + s] = __double2bfloat16(v - (double)__bfloat162float(h));
     }
-    const size_t off = ((size_t)f * P + y) * P + x0;
-    *reinterpret_cast<uint4 *>(hi + off) = *reinterpret_cast<const uint4 *>(h);
-    if (lo) *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(l);
 }

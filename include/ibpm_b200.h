@@ -218,7 +218,7 @@ int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms,
  *     op 0: Lambda = lap_eigs (Δinv_operator, fluid.jl:117-119),
  *     op 1: A at `level`, op 2: Ainv at `level` (A_operator, fluid.jl:121-134);
  *     op 3..5: ops 0..2 with the tensor-core transforms of one BF16 product,
- *     op 6..8: with three products (split BF16); nx = ny in {256, 512, 1024}, FP64
+ *     op 6..8: with three products (split BF16); nx = ny in {256, 512}, FP64
  *     engine only (see ibpm_set_rebuild_transform).
  *   ibpm_diag_apply_B: x = B z (B_operator, coupling.jl:163-176), 2*npanel.
  *   ibpm_diag_binv: the precomputed B^-1 (2np x 2np, column-major); static bodies only. */
@@ -321,12 +321,13 @@ int ibpm_set_warm_start(ibpm_handle *h, int32_t mode, ibpm_net *net, int32_t dep
  * invert (the preconditioner; no counterpart in the reference).  products 0: the
  * FP64 transforms of the step (the default); 1 or 3: every 2D solve of the
  * assembly as four dense DST-I passes on the tensor cores (tcgen05) with BF16
- * operands and FP32 accumulation, one product S_hi x_hi or three
+ * operands and FP32 accumulation (each pass two half-length products by the
+ * transform's even/odd symmetry), one product S_hi x_hi or three
  * (S_hi x_hi + S_hi x_lo + S_lo x_hi, each operand split as hi = bf16(v),
  * lo = bf16(v - hi)).  The preconditioner is then close to, not equal to, the
  * inverse; CG still runs to the same tolerance, so forces are unchanged to
  * that tolerance and only the iteration count can differ.  Moving bodies, FP64
- * engine, nx = ny in {256, 512, 1024}, an sm_100 device; other modes ignore it. */
+ * engine, nx = ny in {256, 512}, an sm_100 device; other modes ignore it. */
 int ibpm_set_rebuild_transform(ibpm_handle *h, int32_t products);
 /* The last step's warm-start features (10 x npanel floats), target (2 x
  * npanel: the converged F~b minus the extrapolated guess x_e) and, in the

@@ -2,8 +2,9 @@
 
 A 2D solve x = S(m ⊙ S(b)) (src/fluid.jl:145-166 with FFTW's RODFT00 as S) runs
 as four dense passes D = S X on tcgen05 with BF16 operands and FP32
-accumulation.  `_emulate` restates that arithmetic in numpy (the same splits,
-roundings and pass order, with round-to-nearest FP32 sums): with one product the
+accumulation, each pass two half-length products by the transform's
+even/odd symmetry.  `_emulate` restates that arithmetic in numpy (the same
+splits, roundings and pass order, with round-to-nearest FP32 sums): with one product the
 GPU result must sit on the emulation, far closer than either sits to the FP64
 solve; with three, whose low parts the accumulator's own rounding reaches, within
 a small factor of the emulation's error.  The preconditioned moving-body modes then assemble B with these solves:
@@ -25,36 +26,53 @@ def _bf16(x):
     return b.astype(np.uint32).view(np.float32)
 
 
+def _split(v):
+    h = _bf16(v)
+    return h, _bf16(np.asarray(v, np.float64) - h)
+
+
+def _uv(X, axis_len):
+    """u (j = 1 .. P/2) and v (j = 1 .. P/2 - 1) of the lines X[line][j - 1]."""
+    P = axis_len
+    h = P // 2
+    j = np.arange(1, h)
+    u = np.concatenate([X[:, j - 1] + X[:, P - j - 1], X[:, h - 1:h]], axis=1)
+    v = X[:, j - 1] - X[:, P - j - 1]
+    return u, v
+
+
 def _emulate(b2, mult, nprod):
-    """The four passes on (P-1)^2 field b2 [y][x] with multipliers mult [ky][kx]."""
+    """The four passes on (P-1)^2 field b2 [y][x] with multipliers mult [ky][kx]:
+    each pass y_k = sum_j S[k][j] u_j (odd k) or v_j (even k) with BF16 operands
+    (split into hi + lo for three products) and FP32 sums, u, v of the lines
+    formed in FP64 from the input and in FP32 between passes."""
     m = b2.shape[0]
     P = m + 1
-    j = np.arange(1, P)
-    S = np.zeros((P, P))
-    S[:m, :m] = 2 * np.sin(np.pi * np.outer(j, j) / P)
-    Sh = _bf16(S)
-    Sl = _bf16(S - Sh)
-    X = np.zeros((P, P))
-    X[:m, :m] = b2
-    Xh = _bf16(X)
-    Xl = _bf16(X - Xh)
+    h = P // 2
+    ko, ke = np.arange(1, P, 2), np.arange(2, P, 2)
+    Ao = 2 * np.sin(np.pi * np.outer(ko, np.arange(1, h + 1)) / P)
+    Ae = 2 * np.sin(np.pi * np.outer(ke, np.arange(1, h)) / P)
+    Aoh, Aol = _split(Ao)
+    Aeh, Ael = _split(Ae)
 
-    def gemm(xh, xl):  # D[k][l] = sum_p S[k][p] X[l][p]
-        D = Sh @ xh.T
+    def prod(Ah, Al, X):  # X: FP64 or FP32 values of the lines' u or v
+        Xh, Xl = _split(X)
+        D = Ah @ Xh.T
         if nprod == 3:
-            D = D + Sh @ xl.T + Sl @ xh.T
+            D = D + Ah @ Xl.T + Al @ Xh.T
         return D.astype(np.float32)
 
-    def split(D):
-        h = _bf16(D)
-        return h, _bf16(D - h)
+    def dpass(X):  # X[line][position], positions 1 .. P-1; returns D[k - 1][line]
+        u, v = _uv(X, P)
+        D = np.zeros((m, X.shape[0]), np.float32)
+        D[ko - 1] = prod(Aoh, Aol, u)
+        D[ke - 1] = prod(Aeh, Ael, v)
+        return D
 
-    D1 = gemm(Xh, Xl)
-    M = np.zeros((P, P), np.float32)
-    M[:m, :m] = mult
-    D2 = (gemm(*split(D1)) * M).astype(np.float32)
-    D4 = gemm(*split(gemm(*split(D2))))
-    return D4[:m, :m].astype(np.float64)
+    D1 = dpass(b2.astype(np.float64))             # [kx][y]
+    D2 = (dpass(D1) * mult).astype(np.float32)    # [ky][kx]
+    D4 = dpass(dpass(D2))                         # [x][ky] -> [y][x]
+    return D4.astype(np.float64)
 
 
 def _rel(a, b):
