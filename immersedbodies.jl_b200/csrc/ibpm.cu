@@ -1195,6 +1195,7 @@ void Engine<T>::assemble_invert_B() {
     const bool rebuilding = uses_binv_start();
     // the preconditioned modes may assemble with the tensor-core transforms
     tc_on = tc_prod > 0 && preconditioned() && tc != nullptr;
+    const bool assembled_tc = tc_on;
     try {
         for (int c0 = 0; c0 < n; c0 += kbatch) {
             const int nb = std::min(kbatch, n - c0);
@@ -1222,6 +1223,13 @@ void Engine<T>::assemble_invert_B() {
         check_launch();
     }
     if (m & 1) CK(cudaMemcpyAsync(Binv, Bwork, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, st));
+    // a B assembled on the tensor cores is nonsymmetric at its rounding level
+    // (1e-5 .. 1e-2); conjugate gradients wants a symmetric preconditioner, so
+    // its inverse is replaced by the symmetric part (M + M^T) / 2
+    if (assembled_tc) {
+        symmetrize_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(Binv, n);
+        check_launch();
+    }
 }
 
 // IBPM_WS_DIRECT's rebuild of B^-1 for the body position of this step, as a graph

@@ -1001,6 +1001,17 @@ static __global__ void gj_block_kernel(const double *__restrict__ S, double *__r
     D[i + (long long)n * j] = v;
 }
 
+// M <- (M + M^T) / 2 in place (n x n, column-major): thread (i, j) with i < j
+// owns both entries of its pair.
+static __global__ void symmetrize_kernel(double *__restrict__ M, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= j || j >= n) return;
+    const double a = M[i + (long long)n * j], b = M[j + (long long)n * i];
+    const double v = 0.5 * (a + b);
+    M[i + (long long)n * j] = v;
+    M[j + (long long)n * i] = v;
+}
+
 // Identity columns [c0, c0+nb) of a 2np-length basis, one per batch.
 static __global__ void unit_columns_kernel(double *__restrict__ f, int n, int c0, int nb) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
