@@ -22,7 +22,8 @@ using ImmersedBodies: State, Problem, CNAB, AbstractSolver, StaticBody, MovingRi
     MovingGrid, n_panels, timestep, gridstep, inc_time_index!, set_time_index!, update_vars!
 import ImmersedBodies: advance!, getstate, create_solver
 
-export GpuCnabSolver, sync!, level_vorticity, level_x_velocity, level_y_velocity, set_warm_start!
+export GpuCnabSolver, sync!, level_vorticity, level_x_velocity, level_y_velocity, set_warm_start!,
+    set_rebuild_transform!
 
 const libibpm = get(ENV, "IBPM_B200_LIB", joinpath(@__DIR__, "..", "lib", "libibpm_b200.so"))
 
@@ -213,12 +214,23 @@ level_y_velocity(solver::GpuCnabSolver, level::Integer=1) =
 # assembled and inverted on the GPU every `depth` steps, FP64 only); plain CG then
 # runs to the configured tolerance.  :preconditioned is :direct with CG
 # preconditioned by that inverse (not the reference's iteration; same stopping
-# rule).  (The learned mode needs a network made with ibpm_net_*.)
+# rule); :preconditioned_extrapolated also starts CG from the stale error
+# extrapolated over the last steps.  (The learned mode needs a network made with
+# ibpm_net_*.)
 function set_warm_start!(solver::GpuCnabSolver, mode::Symbol=:projected; depth::Integer=16)
     m = Dict(:previous => 0, :extrapolated => 2, :projected => 3, :direct => 4, :preconditioned => 5,
         :preconditioned_extrapolated => 6)[mode]
     _check(solver.handle, ccall((:ibpm_set_warm_start, libibpm), Cint, (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32),
         solver.handle, m, C_NULL, depth))
+    solver
+end
+
+# How the preconditioned modes assemble the B they invert: 0 with the step's FP64
+# transforms, 3 (or 1) with dense DST-I passes on the tensor cores of split-BF16
+# (or BF16) operands; nx = ny in {256, 512}.
+function set_rebuild_transform!(solver::GpuCnabSolver, products::Integer=3)
+    _check(solver.handle, ccall((:ibpm_set_rebuild_transform, libibpm), Cint, (Ptr{Cvoid}, Int32),
+        solver.handle, products))
     solver
 end
 
