@@ -77,6 +77,51 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
+def read_tensor_peak():
+    """Dense BF16 TFLOP/s of this pool's B200s for a kernel timed alone (burst)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def tensor_core_rebuild_report(ib, device: int, steps: int = 10, warmup: int = 3):
+    """The preconditioner's B assembled on the tensor cores, rebuilt every step of
+    the moving-body workload (512^2 x 4 levels, 101-point plate, k = 0.55; 202
+    columns per batched solve): steps/s per product count against the FP64
+    direct start (CUDA events on the solver's stream), and, from one profiled
+    step (events around each launch group, eager launches), the tensor-core
+    passes' algorithmic FLOP rate against the measured BF16 peak."""
+    peak, src = read_tensor_peak()
+    out = {"workload": "pitching_plate_512: preconditioned CG rebuilt every step, B assembled from 202 columns; "
+                       "tensor-core passes: 4 nprod P^3 algorithmic flops per field and solve (P = 512)",
+           "fp64_direct_start": direct_start_run(ib, device, steps, warmup, 101, 0)}
+    for products in (3, 1):
+        run = direct_start_run(ib, device, steps, warmup, 101, products)
+        s = ib.GpuCnabSolver(ib.State(ib.configs.pitching_plate(0.55)),
+                             cg=dict(reltol=0.0, abstol=1e-10, maxiter=5000), device=device)
+        s.set_warm_start(None, mode="preconditioned", depth=1)
+        s.set_rebuild_transform(products)
+        for _ in range(2):
+            s.advance_()
+        s.profile(True)
+        s.advance_()
+        n, ms, flops = s.profile_read("tcdst")
+        nl, msl, bytes_l = s.profile_read("tclines")
+        s.profile(False)
+        del s
+        achieved = flops / (ms / 1000.0) / 1e12
+        out[f"products_{products}"] = {
+            "steps_per_s": run["value"], "ms_per_step": run["ms_per_step"],
+            "cg_iterations_mean": run["cg_iterations_mean"],
+            "passes": {"launch_groups": n, "ms": ms, "tflops": flops / 1e12,
+                       "achieved_tflops_s": achieved, "peak_tflops_s": peak, "peak_source": src,
+                       "frac": achieved / peak},
+            "lines": {"launches": nl, "ms": msl, "achieved_gb_s": bytes_l / (msl / 1000.0) / 1e9}}
+    return out
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -451,6 +496,8 @@ def main():
     ap.add_argument("--no-chosen", action="store_true", help="skip the mixed-precision engine")
     ap.add_argument("--no-learned", action="store_true", help="skip the moving-body CG warm-start comparison")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 128-case ensemble measurement")
+    ap.add_argument("--no-tensor-core", action="store_true",
+                    help="skip the tensor-core B rebuild measurement")
     ap.add_argument("--direct-start-only", action="store_true",
                     help="time only the moving-body direct CG start (one JSON line) and exit")
     ap.add_argument("--direct-start-points", type=int, default=101,
@@ -595,6 +642,7 @@ def main():
 
     plate32 = None if args.no_chosen else mixed_precision_plate_report(ib, local)
     learned = None if args.no_learned else warm_start_report(ib, local)
+    tcore = None if args.no_tensor_core else tensor_core_rebuild_report(ib, local)
     ensemble = None if args.no_ensemble else ensemble_report(ib, local, pg, rank, world)
 
     cpu = None
@@ -622,7 +670,7 @@ def main():
                         "steps": e2e_steps, "api": "GpuCnabSolver.advance_ (ctypes -> ibpm_advance + ibpm_get_forces)"},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "chosen_form": chosen, "chosen_form_plate_aoa30": plate32, "learned_warm_start": learned,
-                "ensemble": ensemble}
+                "tensor_core_rebuild": tcore, "ensemble": ensemble}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

@@ -108,7 +108,7 @@ EXPORTS = {
 }
 (IBPM_WS_PREVIOUS, IBPM_WS_LEARNED, IBPM_WS_EXTRAPOLATED, IBPM_WS_PROJECTED, IBPM_WS_DIRECT,
  IBPM_WS_PRECONDITIONED, IBPM_WS_PRECOND_EXTRAP) = 0, 1, 2, 3, 4, 5, 6
-KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5, "tcdst": 6}
+KCLASS = {"xpass": 0, "ypass": 1, "nonlinear": 2, "curl": 3, "xtrial": 4, "ytrial": 5, "tcdst": 6, "tclines": 7}
 
 _lib = None
 

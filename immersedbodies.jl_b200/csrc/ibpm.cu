@@ -744,12 +744,16 @@ struct Engine final : ibpm_handle {
     void tc_solve(const In &in, int nf, const float *mtab, double *out, long long bs,
                   TcKeep keep = TcKeep{TC_KEEP_ALL, nullptr, {0, 0, 0, 0}}) {
         if (!tc || tc_fmax(tc) < nf) throw ApiError{IBPM_ERR_INVALID, "tensor-core transforms not prepared"};
-        const int pe = prof_begin();
+        int pe = prof_begin();
         tc_lines_kernel<In><<<dim3(1, nx, nf), nx / 8, nx * sizeof(double), st>>>(in, nx, tc_in_hi(tc), tc_in_lo(tc));
         check_launch();
+        const double P = nx, parts = tc_nprod(tc) == 3 ? 2 : 1;
+        prof_end(pe, IBPM_KCLASS_TCLINES, (8.0 * ng + 2.0 * parts * P * P) * nf);
+        pe = prof_begin();
         launches += tc_solve_tail(tc, nf, mtab, out, bs, nx - 1, keep, err + 4, st);
         CK(cudaGetLastError());
-        prof_end(pe, IBPM_KCLASS_TCDST, 16.0 * (double)ng * nf);
+        // four passes of nprod half-length products: 4 nprod P^3 flops per field
+        prof_end(pe, IBPM_KCLASS_TCDST, 4.0 * tc_nprod(tc) * P * P * P * nf);
     }
 
     // vort2flux (src/fluid.jl:178-205) over nbatch independent fields.

@@ -207,8 +207,10 @@ int64_t ibpm_kernel_launches(const ibpm_handle *h);
 #define IBPM_KCLASS_CURL 3          /* curl of the streamfunction */
 #define IBPM_KCLASS_XTRIAL 4        /* trial solve, first X pass (all levels) */
 #define IBPM_KCLASS_YTRIAL 5        /* trial solve, Y pass with the A/Ainv multiplies (all levels) */
-#define IBPM_KCLASS_TCDST 6         /* a batched 2D solve on the tensor cores (its five launches) */
-#define IBPM_KCLASS_COUNT 7
+#define IBPM_KCLASS_TCDST 6         /* the four tensor-core passes of a batched 2D solve; its third value
+                                       counts algorithmic flops (4 nprod P^3 per field), not bytes */
+#define IBPM_KCLASS_TCLINES 7       /* the FP64 prologue of a tensor-core solve into BF16 lines */
+#define IBPM_KCLASS_COUNT 8
 int ibpm_profile(ibpm_handle *h, int enable);
 int ibpm_profile_read(ibpm_handle *h, int kclass, int64_t *launches, double *ms, double *bytes);
 
