@@ -670,7 +670,10 @@ def main():
                         "steps": e2e_steps, "api": "GpuCnabSolver.advance_ (ctypes -> ibpm_advance + ibpm_get_forces)"},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "chosen_form": chosen, "chosen_form_plate_aoa30": plate32, "learned_warm_start": learned,
-                "tensor_core_rebuild": tcore, "ensemble": ensemble}
+                "tensor_core_rebuild": tcore, "ensemble": ensemble,
+                "autotune": {"table": ib._abi.tune_table(),
+                             "what": "Y-pass line pairs per block chosen by timing per (GPU, transform length, "
+                                     "precision, batch bucket); every choice gives the same bits"}}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
