@@ -5,7 +5,7 @@
 // (the odd or the even physical indices), over the P/2 slots of the u half (odd
 // frequencies) or the v half (even ones).  It accumulates in TN columns of
 // tensor memory by tcgen05.mma (M 128, N TN, K 16; BF16 x BF16 -> FP32) from
-// K-blocks of 64 elements (128-byte rows, 128-byte swizzle) that TMA brings into
+// K-blocks of 32 elements (64-byte rows, 64-byte swizzle) that TMA brings into
 // a ring of shared-memory stages.  One CTA per SM walks the tiles (M-tiles
 // fastest, so the CTAs working at once share each line tile through L2); two
 // accumulators let the epilogue of one tile run while the products of the next
@@ -30,8 +30,11 @@
 namespace {
 
 constexpr int kTileM = 128;   // rows of A per tile
-constexpr int kBlockK = 64;   // elements per K-block: one 128-byte swizzle row
-constexpr int kBytesA = kTileM * kBlockK * 2;  // 16 KB
+// elements per K-block: one swizzle row of 2 kBlockK bytes (32: 64-byte swizzle;
+// smaller stages keep more of them in flight than 64 with the 128-byte swizzle)
+constexpr int kBlockK = 32;
+constexpr int kRowBytes = 2 * kBlockK;
+constexpr int kBytesA = kTileM * kBlockK * 2;  // 8 KB
 constexpr int kThreads = 192;
 constexpr int kStageLd = 33;
 constexpr int kStageFloats = 32 * kStageLd;
@@ -47,7 +50,7 @@ struct Cfg {
     static constexpr int kBytesB = kTN * kBlockK * 2;
     static constexpr int kParts = NPROD == 3 ? 2 : 1;
     static constexpr int kStageBytes = kParts * (kBytesA + kBytesB);
-    static constexpr int kStages = (192 * 1024) / kStageBytes > 6 ? 6 : (192 * 1024) / kStageBytes;
+    static constexpr int kStages = (192 * 1024) / kStageBytes > 8 ? 8 : (192 * 1024) / kStageBytes;
     static constexpr uint32_t kTmemCols = 2 * kTN;        // two accumulators
     static constexpr int kKB = (P / 2) / kBlockK;          // K-blocks per tile
     // the operand ring, four epilogue staging tiles and alignment slack
@@ -129,13 +132,14 @@ __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, uint
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory operand descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t a) {
+// Shared-memory operand descriptor: K-major, swizzle of one K-block row (64 or
+// 128 bytes), 8-row groups 8 rows apart.
+__device__ __forceinline__ uint64_t sw_desc(uint32_t a) {
     uint64_t d = (uint64_t)((a & 0x3FFFFu) >> 4);
-    d |= (uint64_t)1 << 16;           // leading offset (unused by swizzled K-major layouts)
-    d |= (uint64_t)(1024 >> 4) << 32; // stride between 8-row groups
-    d |= (uint64_t)1 << 46;           // descriptor version
-    d |= (uint64_t)2 << 61;           // 128-byte swizzle
+    d |= (uint64_t)1 << 16;                       // leading offset (unused by swizzled K-major layouts)
+    d |= (uint64_t)((8 * kRowBytes) >> 4) << 32;  // stride between 8-row groups
+    d |= (uint64_t)1 << 46;                       // descriptor version
+    d |= (uint64_t)(kRowBytes == 128 ? 2 : 4) << 61;  // 128-byte or 64-byte swizzle
     return d;
 }
 
@@ -277,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     __shared__ uint64_t full[C::kStages], empty[C::kStages], accf[2], acce[2], fin;
     __shared__ uint32_t tmem_s;
     __shared__ int fail_s;
-    // the 128-byte swizzle atoms must start on 1024-byte boundaries of the shared window
+    // the swizzle atoms (8 rows of one K-block) must start on 1024-byte boundaries of the shared window
     uint8_t *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = nf * MT * NT;
@@ -356,9 +360,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t ah = sw128_desc(saddr(stage_a(s, 0))), bh = sw128_desc(saddr(stage_b(s, 0)));
-                    const uint64_t al = sw128_desc(saddr(stage_a(s, NPROD == 3 ? 1 : 0)));
-                    const uint64_t bl = sw128_desc(saddr(stage_b(s, NPROD == 3 ? 1 : 0)));
+                    const uint64_t ah = sw_desc(saddr(stage_a(s, 0))), bh = sw_desc(saddr(stage_b(s, 0)));
+                    const uint64_t al = sw_desc(saddr(stage_a(s, NPROD == 3 ? 1 : 0)));
+                    const uint64_t bl = sw_desc(saddr(stage_b(s, NPROD == 3 ? 1 : 0)));
 #pragma unroll
                     for (int kk = 0; kk < kBlockK / 16; ++kk) {
                         const uint64_t o = (uint64_t)(kk * 32 >> 4);  // 16 elements = 32 B along the swizzled row
@@ -429,7 +433,7 @@ EncodeTiled encoder() {
     return fn;
 }
 
-// 2D BF16 map over rows x cols (row-major), boxes of box_rows x 64 elements, 128-byte swizzle
+// 2D BF16 map over rows x cols (row-major), boxes of box_rows x kBlockK elements, swizzled like the descriptors
 bool make_map(CUtensorMap *m, void *base, int cols, long long rows, int box_rows) {
     EncodeTiled enc = encoder();
     if (!enc) return false;
@@ -438,7 +442,8 @@ bool make_map(CUtensorMap *m, void *base, int cols, long long rows, int box_rows
     const cuuint32_t box[2] = {(cuuint32_t)kBlockK, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               kRowBytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
