@@ -487,6 +487,8 @@ def run_reference(args, world, rank):
 
 
 def main():
+    # the pass-shape autotuner times its candidates at setup; its choices are in the JSON line
+    os.environ.setdefault("IBPM_TUNE", "1")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
