@@ -118,15 +118,17 @@ __global__ void bbox_kernel(Panels P, Grid g) {
 // faces: the block lists, in panel order, the panels whose support meets the
 // tile, then every face sums w * f over that list in panel order -- the same
 // accumulation order as the reference's sequential loop over panels.
-// f: 2np per batch (x block then y block); patch output per batch.
+// f: 2np per batch (x block then y block); patch output per batch; (bx, by): the
+// tile's place in the bounding box.
 template <class T>
-__device__ __forceinline__ void reg_patch_tile(const Panels &P, const double *__restrict__ fb, T *__restrict__ out) {
+__device__ __forceinline__ void reg_patch_tile(const Panels &P, const double *__restrict__ fb, T *__restrict__ out,
+                                               int bx, int by) {
     __shared__ int list[1024];
     __shared__ int warp_cnt[8];
     __shared__ int total;
     const int i0 = P.bbox[0], i1 = P.bbox[1], j0 = P.bbox[2], j1 = P.bbox[3];
     const int pw = i1 - i0 + 1, ph = j1 - j0 + 1;
-    const int ti0 = i0 + blockIdx.x * kTile, tj0 = j0 + blockIdx.y * kTile;
+    const int ti0 = i0 + bx * kTile, tj0 = j0 + by * kTile;
     if (ti0 > i1 || tj0 > j1) return;
     const int ti1 = min(ti0 + kTile - 1, i1), tj1 = min(tj0 + kTile - 1, j1);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -179,7 +181,10 @@ template <class T>
 __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *__restrict__ f, long long fbs,
                                                         T *__restrict__ patch, long long pbs) {
     const int b = blockIdx.z;
-    reg_patch_tile<T>(P, f + b * fbs, patch + b * pbs);
+    // the blocks walk the tiles of the bounding box (its size is known on the device only)
+    const int pw = P.bbox[1] - P.bbox[0] + 1, ph = P.bbox[3] - P.bbox[2] + 1;
+    for (int by = blockIdx.y; by * kTile < ph; by += gridDim.y)
+        for (int bx = blockIdx.x; bx * kTile < pw; bx += gridDim.x) reg_patch_tile<T>(P, f + b * fbs, patch + b * pbs, bx, by);
 }
 
 // reg_patch_kernel for the cases of a batched ensemble group (case = blockIdx.z):
@@ -187,7 +192,10 @@ __global__ void __launch_bounds__(256) reg_patch_kernel(Panels P, const double *
 template <class T>
 __global__ void __launch_bounds__(256) reg_patch_multi_kernel(const CaseView *__restrict__ tab) {
     const CaseView &cv = tab[blockIdx.z];
-    reg_patch_tile<T>(cv.P, cv.Fbt, static_cast<T *>(cv.patch));
+    const int pw = cv.P.bbox[1] - cv.P.bbox[0] + 1, ph = cv.P.bbox[3] - cv.P.bbox[2] + 1;
+    for (int by = blockIdx.y; by * kTile < ph; by += gridDim.y)
+        for (int bx = blockIdx.x; bx * kTile < pw; bx += gridDim.x)
+            reg_patch_tile<T>(cv.P, cv.Fbt, static_cast<T *>(cv.patch), bx, by);
 }
 
 // regT! (src/coupling.jl:57-69): fb[p, c] = dot(q_c[7x7 at p], w[p, c]) in
@@ -271,11 +279,18 @@ void launch_reg_weights(const Panels &P, int p0, int p1, const Grid &g, cudaStre
     if (p1 > p0) reg_weights_kernel<<<p1 - p0, dim3(49, 2), 0, st>>>(P, p0, g);
 }
 void launch_bbox(const Panels &P, const Grid &g, cudaStream_t st) { bbox_kernel<<<1, 256, 0, st>>>(P, g); }
+// Blocks per dimension for the patch kernels: with many batches, enough for a
+// bounding box of 128 faces in one sweep (a larger box takes more sweeps); with
+// a few, the tiles of the whole grid, each block at most one tile.
+static int patch_grid(int n, int nbatch) {
+    const int whole = (n + 1 + kTile - 1) / kTile + 1;
+    return nbatch > 4 && whole > 8 ? 8 : whole;
+}
+
 template <class T>
 void launch_reg_patch(const Panels &P, const double *f, long long fbs, T *patch, long long pbs, int nbatch,
                       const Grid &g, cudaStream_t st) {
-    const int tiles_x = (g.nx + 1 + kTile - 1) / kTile + 1, tiles_y = (g.ny + 1 + kTile - 1) / kTile + 1;
-    reg_patch_kernel<T><<<dim3(tiles_x, tiles_y, nbatch), 256, 0, st>>>(P, f, fbs, patch, pbs);
+    reg_patch_kernel<T><<<dim3(patch_grid(g.nx, nbatch), patch_grid(g.ny, nbatch), nbatch), 256, 0, st>>>(P, f, fbs, patch, pbs);
 }
 template <class T>
 void launch_regT(const Panels &P, const T *q, long long qbs, double *out, long long obs, int nbatch, int add_q0,
@@ -286,8 +301,7 @@ void launch_regT(const Panels &P, const T *q, long long qbs, double *out, long l
 }
 template <class T>
 void launch_reg_patch_multi(const CaseView *tab, int ncase, const Grid &g, cudaStream_t st) {
-    const int tiles_x = (g.nx + 1 + kTile - 1) / kTile + 1, tiles_y = (g.ny + 1 + kTile - 1) / kTile + 1;
-    reg_patch_multi_kernel<T><<<dim3(tiles_x, tiles_y, ncase), 256, 0, st>>>(tab);
+    reg_patch_multi_kernel<T><<<dim3(patch_grid(g.nx, ncase), patch_grid(g.ny, ncase), ncase), 256, 0, st>>>(tab);
 }
 template <class T>
 void launch_regT_multi(const CaseView *tab, int ncase, int np_max, const T *q, long long qbs, const StepDev *prm,

@@ -816,7 +816,11 @@ struct Engine final : ibpm_handle {
             }
             if (curl_all || lev == 1) {
                 const dim3 blk(64, 4);
-                const dim3 grd((nx + 1 + 63) / 64, (ny + 1 + 3) / 4, nbatch);
+                // with a window and many fields the blocks sweep it (128 x 128 faces per
+                // sweep); a few fields keep one thread per face of the whole grid
+                const bool windowed = lev == 1 && win != nullptr && nbatch > 4;
+                const dim3 grd(windowed ? std::min(2, (nx + 1 + 63) / 64) : (nx + 1 + 63) / 64,
+                               windowed ? std::min(32, (ny + 1 + 3) / 4) : (ny + 1 + 3) / 4, nbatch);
                 const int pe = prof_begin();
                 curl_kernel<T, T, T><<<grd, blk, 0, st>>>(qout + (lev - 1) * nq, qbs, Pl, bs,
                                                           lev < L ? psi_ + lev * ng : nullptr, bs, g,

@@ -691,55 +691,63 @@ __global__ void __launch_bounds__(kNlTX *kNlBY, EXT ? 4 : 5) nonlinear_kernel(No
 // One thread per (i, j) writes both faces there: the x face u(i, j) (i <= nx+1,
 // j <= ny) and the y face v(i, j) (i <= nx, j <= ny+1); inside the ring they share
 // psi(i-1, j-1).  Batch b (blockIdx.z) uses psi + b*bs, q + b*qbs, coarse + b*cbs.
-// win (device, may be null): only the faces in i0..i1 x j0..j1 are written.
+// win (device, may be null): only the faces in i0..i1 x j0..j1 are written, by a
+// grid of any size sweeping the window.
 template <class T, class TP, class TC>
 __global__ void curl_kernel(T *__restrict__ qout, long long qbs, const TP *__restrict__ psi, long long bs,
                             const TC *__restrict__ coarse, long long cbs, Grid g, const int *__restrict__ win = nullptr) {
     const int nx = g.nx, ny = g.ny;
     const long long nu = (long long)(nx + 1) * ny;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int b = blockIdx.z;
-    if (i > nx + 1 || j > ny + 1) return;
-    if (win != nullptr && (i < win[0] || i > win[1] || j < win[2] || j > win[3])) return;
     const TP *Pt = psi + b * bs;
     const TC *C = coarse ? coarse + b * cbs : nullptr;
     T *q = qout + b * qbs;
     auto P = [&](long long k) -> double { return (double)Pt[k]; };
-    if (i >= 2 && i <= nx - 1 && j >= 2 && j <= ny - 1) {
-        const double pc = P(GI(i - 1, j - 1));
-        q[UI(i, j)] = (T)(P(GI(i - 1, j)) - pc);
-        q[VI(i, j)] = (T)(pc - P(GI(i, j - 1)));
+    auto face = [&](int i, int j) {
+        if (i >= 2 && i <= nx - 1 && j >= 2 && j <= ny - 1) {
+            const double pc = P(GI(i - 1, j - 1));
+            q[UI(i, j)] = (T)(P(GI(i - 1, j)) - pc);
+            q[VI(i, j)] = (T)(pc - P(GI(i, j - 1)));
+            return;
+        }
+        if (j <= ny) {
+            double v;
+            if (i == 1)
+                v = getbc(C, g, SIDE_L, j + 1) - getbc(C, g, SIDE_L, j);
+            else if (i == nx + 1)
+                v = getbc(C, g, SIDE_R, j + 1) - getbc(C, g, SIDE_R, j);
+            else if (j == 1)
+                v = P(GI(i - 1, 1)) - getbc(C, g, SIDE_B, i);
+            else if (j == ny)
+                v = getbc(C, g, SIDE_T, i) - P(GI(i - 1, ny - 1));
+            else
+                v = P(GI(i - 1, j)) - P(GI(i - 1, j - 1));
+            q[UI(i, j)] = (T)v;
+        }
+        if (i <= nx) {
+            double v;
+            if (j == 1)
+                v = getbc(C, g, SIDE_B, i) - getbc(C, g, SIDE_B, i + 1);
+            else if (j == ny + 1)
+                v = getbc(C, g, SIDE_T, i) - getbc(C, g, SIDE_T, i + 1);
+            else if (i == 1)
+                v = getbc(C, g, SIDE_L, j) - P(GI(1, j - 1));
+            else if (i == nx)
+                v = P(GI(nx - 1, j - 1)) - getbc(C, g, SIDE_R, j);
+            else
+                v = P(GI(i - 1, j - 1)) - P(GI(i, j - 1));
+            q[VI(i, j)] = (T)v;
+        }
+    };
+    const int ti = blockIdx.x * blockDim.x + threadIdx.x, tj = blockIdx.y * blockDim.y + threadIdx.y;
+    if (win == nullptr) {
+        if (ti + 1 <= nx + 1 && tj + 1 <= ny + 1) face(ti + 1, tj + 1);
         return;
     }
-    if (j <= ny) {
-        double v;
-        if (i == 1)
-            v = getbc(C, g, SIDE_L, j + 1) - getbc(C, g, SIDE_L, j);
-        else if (i == nx + 1)
-            v = getbc(C, g, SIDE_R, j + 1) - getbc(C, g, SIDE_R, j);
-        else if (j == 1)
-            v = P(GI(i - 1, 1)) - getbc(C, g, SIDE_B, i);
-        else if (j == ny)
-            v = getbc(C, g, SIDE_T, i) - P(GI(i - 1, ny - 1));
-        else
-            v = P(GI(i - 1, j)) - P(GI(i - 1, j - 1));
-        q[UI(i, j)] = (T)v;
-    }
-    if (i <= nx) {
-        double v;
-        if (j == 1)
-            v = getbc(C, g, SIDE_B, i) - getbc(C, g, SIDE_B, i + 1);
-        else if (j == ny + 1)
-            v = getbc(C, g, SIDE_T, i) - getbc(C, g, SIDE_T, i + 1);
-        else if (i == 1)
-            v = getbc(C, g, SIDE_L, j) - P(GI(1, j - 1));
-        else if (i == nx)
-            v = P(GI(nx - 1, j - 1)) - getbc(C, g, SIDE_R, j);
-        else
-            v = P(GI(i - 1, j - 1)) - P(GI(i, j - 1));
-        q[VI(i, j)] = (T)v;
-    }
+    // the window (known on the device only) in grid-strided sweeps of a smaller grid
+    const int i1 = min(win[1], nx + 1), j1 = min(win[3], ny + 1);
+    for (int j = max(win[2], 1) + tj; j <= j1; j += gridDim.y * blockDim.y)
+        for (int i = max(win[0], 1) + ti; i <= i1; i += gridDim.x * blockDim.x) face(i, j);
 }
 
 // coarsify! (src/fluid.jl:208-228): fine level -> central block of the next coarser level

@@ -23,6 +23,7 @@
 // significant bits per operand).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -86,12 +87,39 @@ __device__ __forceinline__ void tc_split(float v, __nv_bfloat16 &hi, __nv_bfloat
 // once, coalesced, into shared memory (P doubles); thread t then forms slots t,
 // t + P/8, ... (neighbouring threads read neighbouring pairs).  Block: P / 8
 // threads; grid (1, P, nf); P * 8 bytes of shared memory.
+// A prologue with kSplitRing = true offers plain(f, i, j), the field alone, and
+// ring(v, f, i, j), v plus its boundary values on the outer ring (in the same
+// order as its operator()); the row is then loaded plainly first and the few
+// ring elements completed after, so no load of the row waits behind the
+// boundary reads.
+template <class In, class = void>
+struct TcSplitRing {
+    static constexpr bool value = false;
+};
+template <class In>
+struct TcSplitRing<In, std::void_t<decltype(In::kSplitRing)>> {
+    static constexpr bool value = In::kSplitRing;
+};
+
 template <class In>
 __global__ void tc_lines_kernel(In in, int P, __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
     extern __shared__ double tc_row[];
     const int f = blockIdx.z, l = blockIdx.y, t = threadIdx.x, nt = blockDim.x;
     const int y = tc_blk(l, P);
-    for (int x = t + 1; x < P; x += nt) tc_row[x] = y != 0 ? in(f, x, y) : 0.0;
+    if constexpr (TcSplitRing<In>::value) {
+        for (int x = t + 1; x < P; x += nt) tc_row[x] = y != 0 ? in.plain(f, x, y) : 0.0;
+        __syncthreads();
+        if (y != 0) {
+            if (in.ring_row(y)) {
+                for (int x = t + 1; x < P; x += nt) tc_row[x] = in.ring(tc_row[x], f, x, y);
+            } else if (t < 2) {
+                const int x = t == 0 ? 1 : P - 1;
+                tc_row[x] = in.ring(tc_row[x], f, x, y);
+            }
+        }
+    } else {
+        for (int x = t + 1; x < P; x += nt) tc_row[x] = y != 0 ? in(f, x, y) : 0.0;
+    }
     __syncthreads();
     const size_t off = ((size_t)f * P + l) * P;
     for (int s = t; s < P; s += nt) {
