@@ -1217,10 +1217,10 @@ void Engine<T>::assemble_invert_B() {
     }
     tc_on = false;
     // n = 2 np is even: n / 2 two-step launches, or for the moving-body rebuilds
-    // (rebuilding) eight steps per launch as one block pivot; after an odd count
+    // (rebuilding) kGJB steps per launch as one block pivot; after an odd count
     // of launches the result is in Bwork
     int m = 0;
-    const int step = rebuilding ? 8 : 2;
+    const int step = rebuilding ? kGJB : 2;
     for (int k = 0; k < n; k += step, ++m) {
         const double *src = (m & 1) ? Bwork : Binv;
         double *dst = (m & 1) ? Binv : Bwork;

@@ -941,28 +941,30 @@ static __global__ void gj_step2_kernel(const double *__restrict__ S, double *__r
     D[i + (long long)n * j] = v;
 }
 
-// Steps k .. k + b - 1 (b <= 8) of the same elimination in one launch, as one
+// Steps k .. k + b - 1 (b <= kGJB) of the same elimination in one launch, as one
 // block pivot: with K = {k .. k + b - 1}, P = S_KK^-1 (formed here by b
 // unpivoted steps on the b x b block),
 //   D_KK = P, D_KR = P S_KR, D_RK = -S_RK P, D_RR = S_RR - S_RK P S_KR,
 // which equals the b single steps in exact arithmetic (not bit for bit).  One
 // block per column j, threads over rows i (n <= blockDim.x * gridDim.x).  A
 // pivot <= 0 sets *err to its step + 1.
+constexpr int kGJB = 16;  // steps per block-pivot launch (blockDim >= kGJB^2)
 static __global__ void gj_block_kernel(const double *__restrict__ S, double *__restrict__ D, int n, int k, int b,
                                        int *err) {
-    __shared__ double Pm[8][8];
-    __shared__ double T[8];  // P S_Kj for this block's column j
+    __shared__ double Pm[kGJB][kGJB];
+    __shared__ double T[kGJB];  // P S_Kj for this block's column j
     const int j = blockIdx.y, t = threadIdx.x;
-    if (t < 64) {
-        const int a = t / 8, c = t % 8;
+    constexpr int kE = kGJB * kGJB;
+    if (t < kE) {
+        const int a = t / kGJB, c = t % kGJB;
         Pm[a][c] = (a < b && c < b) ? S[(k + a) + (long long)n * (k + c)] : 0.0;
     }
     __syncthreads();
-    // in-place unpivoted Gauss-Jordan of the b x b block, thread t < 64 owning (t / 8, t % 8)
-    const int a = t / 8, c = t % 8;
+    // in-place unpivoted Gauss-Jordan of the b x b block, thread t < kGJB^2 owning (t / kGJB, t % kGJB)
+    const int a = t / kGJB, c = t % kGJB;
     for (int q = 0; q < b; ++q) {
         double p = 0.0, aq = 0.0, qc = 0.0, ac = 0.0;
-        if (t < 64) {
+        if (t < kE) {
             p = Pm[q][q];
             aq = Pm[a][q];
             qc = Pm[q][c];
@@ -970,7 +972,7 @@ static __global__ void gj_block_kernel(const double *__restrict__ S, double *__r
         }
         __syncthreads();
         if (t == 0 && blockIdx.x == 0 && j == 0 && !(p > 0.0)) atomicCAS(err, 0, k + q + 1);
-        if (t < 64 && a < b && c < b) {
+        if (t < kE && a < b && c < b) {
             const double ip = 1.0 / p;
             if (a == q && c == q)
                 Pm[a][c] = ip;
