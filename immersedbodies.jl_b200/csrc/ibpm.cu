@@ -629,65 +629,67 @@ struct Engine final : ibpm_handle {
     // Merged trial solve over all L levels: Gamma_new = Ainv(A Gamma + rest)
     // nb batches of ng (L for one case; cases x L for an ensemble group, whose
     // per-batch coefficients dt / (2 Re hc^2) come from ctab)
-    template <class D>
-    void trial_t(const T *Gold, const T *rest_, T *Gnew, int nb, const double *ctab) {
-        trial_core<D>(Gold, rest_, Gnew, nb, ctab, t1, t2, rhs, plx, ply);
-    }
-    // the merged trial solve on fields of the transform's element type R, with
-    // scratch t1_, t2_, rhs_ (nb fields each) and the plans of R
+    // The merged trial solve on fields of element type R, with scratch t1_, t2_,
+    // rhs_ (nb fields each) and the plans of R: the first X pass and the Y pass
+    // each take the compile-time transform of their own length (nx and ny may
+    // differ), then the plain X pass.
     template <class D, class R = typename D::Real>
+    void trial_xpart(const R *Gold, const R *rest_, int nb, R *t1_, R *t2_, const PlanT<R> &px) {
+        const dim3 grid((ny - 1 + kNG - 1) / kNG, nb);
+        const size_t sm = pass_smem<D>(px.M, kNG, kNG);
+        const int pe = prof_begin();
+        xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1_, t2_, ng, nx - 1, px, ny - 1);
+        check_launch();
+        prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(R) * (double)ng * nb);
+    }
+    template <class D, class R = typename D::Real>
+    void trial_ypart(int nb, const double *ctab, R *t1_, R *t2_, R *rhs_, const PlanT<R> &py) {
+        const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nb);
+        const size_t sm = pass_smem<D>(py.M, 2 * kNG, kNG);
+        // the cap must cover the largest M this instantiation serves (kMaxM); the
+        // attribute is per device
+        static std::atomic<unsigned long long> attr_devices{0};
+        if (need_attr(attr_devices)) {
+            const int cap = (int)pass_smem<D>(kMaxM, 2 * kNG, kNG);
+            CK(cudaFuncSetAttribute(ypass_trial_kernel<D, kNG>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+            attr_devices.fetch_or(device_bit());
+        }
+        const int pe = prof_begin();
+        Mult m = mult(MULT_AIMPL, 1, 1);
+        m.coef_tab = ctab;
+        ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1_, t2_, rhs_, ng, nx - 1, py, m);
+        check_launch();
+        prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(R) * (double)ng * nb);
+    }
+    template <class R>
     void trial_core(const R *Gold, const R *rest_, R *Gnew, int nb, const double *ctab, R *t1_, R *t2_, R *rhs_,
                     const PlanT<R> &px, const PlanT<R> &py) {
-        {
-            const dim3 grid((ny - 1 + kNG - 1) / kNG, nb);
-            const size_t sm = pass_smem<D>(px.M, kNG, kNG);
-            const int pe = prof_begin();
-            xpass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(Gold, rest_, t1_, t2_, ng, nx - 1, px, ny - 1);
-            check_launch();
-            prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(R) * (double)ng * nb);
+        switch (px.M) {
+            case 1024: trial_xpart<Pow2Dst<1024, R>>(Gold, rest_, nb, t1_, t2_, px); break;
+            case 512: trial_xpart<Pow2Dst<512, R>>(Gold, rest_, nb, t1_, t2_, px); break;
+            case 256: trial_xpart<Pow2Dst<256, R>>(Gold, rest_, nb, t1_, t2_, px); break;
+            case 384: trial_xpart<MixDst<384, R>>(Gold, rest_, nb, t1_, t2_, px); break;
+            default: trial_xpart<GenericDst<R>>(Gold, rest_, nb, t1_, t2_, px); break;
         }
-        {
-            const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nb);
-            const size_t sm = pass_smem<D>(py.M, 2 * kNG, kNG);
-            // the cap must cover the largest M this instantiation serves (kMaxM); the
-            // attribute is per device
-            static std::atomic<unsigned long long> attr_devices{0};
-            if (need_attr(attr_devices)) {
-                const int cap = (int)pass_smem<D>(kMaxM, 2 * kNG, kNG);
-                CK(cudaFuncSetAttribute(ypass_trial_kernel<D, kNG>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-                attr_devices.fetch_or(device_bit());
-            }
-            const int pe = prof_begin();
-            Mult m = mult(MULT_AIMPL, 1, 1);
-            m.coef_tab = ctab;
-            ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1_, t2_, rhs_, ng, nx - 1, py, m);
-            check_launch();
-            prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(R) * (double)ng * nb);
+        switch (py.M) {
+            case 1024: trial_ypart<Pow2Dst<1024, R>>(nb, ctab, t1_, t2_, rhs_, py); break;
+            case 512: trial_ypart<Pow2Dst<512, R>>(nb, ctab, t1_, t2_, rhs_, py); break;
+            case 256: trial_ypart<Pow2Dst<256, R>>(nb, ctab, t1_, t2_, rhs_, py); break;
+            case 384: trial_ypart<MixDst<384, R>>(nb, ctab, t1_, t2_, rhs_, py); break;
+            default: trial_ypart<GenericDst<R>>(nb, ctab, t1_, t2_, rhs_, py); break;
         }
         xpass<R>(InPlain<R>{rhs_, ng, nx - 1}, OutPlain<R>{Gnew, ng, nx - 1}, nb);
     }
     // the merged trial solve of one FP64 level (IBPM_MIXED_L1's level 1)
     void trial_d(const double *Gold, const double *rest_, double *Gnew) {
-        const PlanT<double> &px = plan_x<double>(), &py = plan_y<double>();
-        if (px.M == 1024 && py.M == 1024)
-            trial_core<Pow2Dst<1024, double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
-        else if (px.M == 512 && py.M == 512)
-            trial_core<Pow2Dst<512, double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
-        else if (px.M == 256 && py.M == 256)
-            trial_core<Pow2Dst<256, double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
-        else
-            trial_core<GenericDst<double>>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, px, py);
+        trial_core<double>(Gold, rest_, Gnew, 1, nullptr, t1d, t2d, rhsd, plan_x<double>(), plan_y<double>());
     }
+    // Merged trial solve over all L levels: Gamma_new = Ainv(A Gamma + rest)
+    // nb batches of ng (L for one case; cases x L for an ensemble group, whose
+    // per-batch coefficients dt / (2 Re hc^2) come from ctab)
     void trial(const T *Gold, const T *rest_, T *Gnew, int nb = 0, const double *ctab = nullptr) {
         if (nb == 0) nb = L;
-        if (plx.M == 1024 && ply.M == 1024)
-            trial_t<Pow2Dst<1024, T>>(Gold, rest_, Gnew, nb, ctab);
-        else if (plx.M == 512 && ply.M == 512)
-            trial_t<Pow2Dst<512, T>>(Gold, rest_, Gnew, nb, ctab);
-        else if (plx.M == 256 && ply.M == 256)
-            trial_t<Pow2Dst<256, T>>(Gold, rest_, Gnew, nb, ctab);
-        else
-            trial_t<GenericDst<T>>(Gold, rest_, Gnew, nb, ctab);
+        trial_core<T>(Gold, rest_, Gnew, nb, ctab, t1, t2, rhs, plx, ply);
     }
 
     Mult mult(int mode, int lev0, int levstep) const {
