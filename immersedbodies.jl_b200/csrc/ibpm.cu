@@ -2044,6 +2044,11 @@ void Engine<T>::set_rebuild_transform(int products) {
         binv_exec = nullptr;
         binv_graph = nullptr;
     }
+    // back to the FP64 transforms: the plan's line buffers are released
+    if (products == 0 && tc) {
+        tc_destroy(tc);
+        tc = nullptr;
+    }
     tc_prod = products;
 }
 
