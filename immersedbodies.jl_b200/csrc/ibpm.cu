@@ -642,22 +642,29 @@ struct Engine final : ibpm_handle {
         check_launch();
         prof_end(pe, IBPM_KCLASS_XTRIAL, 4.0 * sizeof(R) * (double)ng * nb);
     }
-    template <class D, class R = typename D::Real>
+    template <class D, int NG = kNG, class R = typename D::Real>
     void trial_ypart(int nb, const double *ctab, R *t1_, R *t2_, R *rhs_, const PlanT<R> &py) {
-        const dim3 grid((nx - 1 + 2 * kNG - 1) / (2 * kNG), nb);
-        const size_t sm = pass_smem<D>(py.M, 2 * kNG, kNG);
+        // many fields per launch (ensemble groups) take 2 NG columns per block
+        if constexpr (NG == kNG) {
+            if (nb >= 16 && py.M <= 512) {
+                trial_ypart<D, 2 * kNG>(nb, ctab, t1_, t2_, rhs_, py);
+                return;
+            }
+        }
+        const dim3 grid((nx - 1 + 2 * NG - 1) / (2 * NG), nb);
+        const size_t sm = pass_smem<D>(py.M, 2 * NG, NG);
         // the cap must cover the largest M this instantiation serves (kMaxM); the
         // attribute is per device
         static std::atomic<unsigned long long> attr_devices{0};
         if (need_attr(attr_devices)) {
-            const int cap = (int)pass_smem<D>(kMaxM, 2 * kNG, kNG);
-            CK(cudaFuncSetAttribute(ypass_trial_kernel<D, kNG>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+            const int cap = (int)pass_smem<D>(kMaxM, 2 * NG, NG);
+            CK(cudaFuncSetAttribute(ypass_trial_kernel<D, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
             attr_devices.fetch_or(device_bit());
         }
         const int pe = prof_begin();
         Mult m = mult(MULT_AIMPL, 1, 1);
         m.coef_tab = ctab;
-        ypass_trial_kernel<D, kNG><<<grid, kNG * D::TPF, sm, st>>>(t1_, t2_, rhs_, ng, nx - 1, py, m);
+        ypass_trial_kernel<D, NG><<<grid, NG * D::TPF, sm, st>>>(t1_, t2_, rhs_, ng, nx - 1, py, m);
         check_launch();
         prof_end(pe, IBPM_KCLASS_YTRIAL, 3.0 * sizeof(R) * (double)ng * nb);
     }
