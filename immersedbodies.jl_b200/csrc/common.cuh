@@ -81,6 +81,20 @@ __device__ __forceinline__ double apply_bc_at(double v, const T *__restrict__ r,
     return v;
 }
 
+// One element global -> shared memory without passing through registers
+// (cp.async, 4 or 8 bytes; both addresses naturally aligned).  Completed by
+// cp_async_wait_all() in the issuing thread, then a barrier for the block.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T *sdst, const T *gsrc) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ bool on_ring(const Grid &g, int i, int j) {
     return j == 1 || j == g.ny - 1 || i == 1 || i == g.nx - 1;
 }

@@ -202,7 +202,13 @@ int tune_forced_ng() {
 // The C ABI's opaque handle: one engine of either precision.
 struct ibpm_handle {
     std::string last_error;
-    virtual ~ibpm_handle() {}
+    // the ensembles holding this case, told when it is destroyed, so that an
+    // ensemble destroyed after its cases (any order of destruction) never
+    // touches them
+    std::vector<std::pair<ibpm_ensemble *, void (*)(ibpm_ensemble *, ibpm_handle *)>> holders;
+    virtual ~ibpm_handle() {
+        for (auto &w : holders) w.second(w.first, this);
+    }
     virtual void set_state(const ibpm_state_view *s) = 0;
     virtual void get_state(ibpm_state_view *s) = 0;
     virtual void get_field(int field, int level, double *out) = 0;
@@ -2536,6 +2542,14 @@ struct CaseGroup {
         }
     }
 
+    // a member destroyed while grouped: its slot is never touched again (the
+    // group cannot step any more; the ensemble refuses to)
+    void forget(const ibpm_handle *h) {
+        for (auto &x : cs)
+            if (x != nullptr && static_cast<const ibpm_handle *>(x) == h) x = nullptr;
+        if (e0 != nullptr && static_cast<const ibpm_handle *>(e0) == h) e0 = nullptr;
+    }
+
     // copies every case back into buffers of its own (before the group's memory goes)
     void unbind() {
         if (cs.empty()) return;
@@ -2543,6 +2557,7 @@ struct CaseGroup {
         CK(cudaStreamSynchronize(st));
         const size_t ngL = (size_t)(ng * L), nqL = (size_t)(nq * L);
         for (int c = 0; c < C; ++c) {
+            if (cs[c] == nullptr) continue;
             Engine<T> &e = *cs[c];
             CK(cudaStreamSynchronize(e.st));
             e.drop_graphs();
@@ -2881,13 +2896,29 @@ int ibpm_advance(ibpm_handle *h, int64_t nsteps, const ibpm_step_params *params)
 
 struct ibpm_ensemble {
     std::vector<ibpm_handle *> cases;
+    std::vector<char> gone;  // cases destroyed while the ensemble lives
     std::string last_error;
     std::vector<std::unique_ptr<CaseGroup<double>>> g64;
     std::vector<std::unique_ptr<CaseGroup<float>>> g32;
     std::vector<std::vector<int>> members64, members32;  // case indices of each group
     std::vector<int> alone;                              // cases stepped on their own streams
+    static void case_gone(ibpm_ensemble *e, ibpm_handle *h) {
+        for (size_t c = 0; c < e->cases.size(); ++c)
+            if (e->cases[c] == h) e->gone[c] = 1;
+        for (auto &g : e->g64) g->forget(h);
+        for (auto &g : e->g32) g->forget(h);
+    }
+    void hold() {
+        gone.assign(cases.size(), 0);
+        for (ibpm_handle *h : cases) h->holders.push_back({this, &ibpm_ensemble::case_gone});
+    }
     ~ibpm_ensemble() {
-        g64.clear();  // each group copies its cases back into buffers of their own
+        for (size_t c = 0; c < cases.size(); ++c) {
+            if (c < gone.size() && gone[c]) continue;
+            auto &v = cases[c]->holders;
+            v.erase(std::remove_if(v.begin(), v.end(), [&](const auto &w) { return w.first == this; }), v.end());
+        }
+        g64.clear();  // each group copies its live cases back into buffers of their own
         g32.clear();
     }
 };
@@ -2949,6 +2980,7 @@ int ibpm_ensemble_create(ibpm_handle *const *cases, int32_t n, ibpm_ensemble **o
     }
     ibpm_ensemble *e = new ibpm_ensemble;
     e->cases.assign(cases, cases + n);
+    e->hold();
     bool batch = true;
     if (const char *v = getenv("IBPM_ENSEMBLE_BATCH")) batch = v[0] != '0';
     std::vector<bool> taken(n, false);
@@ -2975,6 +3007,11 @@ void ibpm_ensemble_destroy(ibpm_ensemble *e) { delete e; }
 // its own stream, all enqueued before any is waited for.
 int ibpm_ensemble_advance(ibpm_ensemble *e, int64_t nsteps, const ibpm_step_params *params) {
     if (!e || nsteps < 0 || (nsteps > 0 && !params)) return IBPM_ERR_INVALID;
+    for (char d : e->gone)
+        if (d) {
+            e->last_error = "a case of the ensemble was destroyed before it";
+            return IBPM_ERR_INVALID;
+        }
     const int64_t n = (int64_t)e->cases.size();
     auto finish_all = [&] {
         for (auto &g : e->g64) guarded(nullptr, [&] { g->finish(); });

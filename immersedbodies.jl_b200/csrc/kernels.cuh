@@ -553,31 +553,17 @@ struct NonlinArgs {
     const TC *coarse = nullptr;
 };
 
-template <class T, class TC>
-__device__ __forceinline__ double avg_qx(const NonlinArgs<T, TC> &a, const StepDev *prm, const T *q, int lev, int i,
-                                         int j) {
-    const Grid &g = a.g;
-    return ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + base_flux_x(g, prm, lev, i, j) +
-            base_flux_x(g, prm, lev, i, j - 1)) / 2;
-}
-template <class T, class TC>
-__device__ __forceinline__ double avg_qy(const NonlinArgs<T, TC> &a, const StepDev *prm, const T *q, long long nu,
-                                         int lev, int i, int j) {
-    const Grid &g = a.g;
-    return ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + base_flux_y(g, prm, lev, i, j) +
-            base_flux_y(g, prm, lev, i - 1, j)) / 2;
-}
-
 // Tile of the nonlinear kernel: kNlTX x kNlTY circulation points per block of
 // kNlTX x kNlBY threads (two rows of outputs per thread).
 constexpr int kNlTX = 32, kNlTY = 16, kNlBY = 8;
 
 // nonlinear (src/fluid.jl:340-455) fused with the rhs assembly of
 // get_trial_state (src/fluid.jl:487-493), all levels (blockIdx.z) at once.
-// Every face average Q = (q + q0) pair sum / 2 (avg_flux!) and every Gamma of the
-// tile and its one-point halo is read once into shared memory; each flux product
-// (direct_product_loops!) and the rot! difference are then formed from there, with
-// the reference's expressions, so each value rounds exactly as in a direct
+// The tile's faces, Gamma (with a one-point halo) and N2 are copied to shared
+// memory with cp.async, all in flight at once; every face average Q = (q + q0)
+// pair sum / 2 (avg_flux!) is then formed once per tile, and each flux product
+// (direct_product_loops!) and the rot! difference from there, with the
+// reference's expressions, so each value rounds exactly as in a direct
 // evaluation.
 // EXT: the ensemble / mixed-precision features of NonlinArgs (levels from lev0,
 // per-case tables, a coarse field of another type); without them the kernel
@@ -610,23 +596,70 @@ __global__ void __launch_bounds__(kNlTX *kNlBY, EXT ? 4 : 5) nonlinear_kernel(No
     }
     __shared__ double aqy[kNlTY + 2][kNlTX];      // avg_qy(i, j), i = I0+2+x, j = J0+1+y
     __shared__ double aqx[kNlTY][kNlTX + 2];      // avg_qx(i, j), i = I0+1+x, j = J0+2+y
-    __shared__ double gm[kNlTY + 2][kNlTX + 2];   // Gamma(i, j),  i = I0+x,   j = J0+y
+    __shared__ T gm[kNlTY + 2][kNlTX + 2];        // Gamma(i, j),  i = I0+x,   j = J0+y
+    __shared__ T ru[kNlTY + 1][kNlTX + 2];        // q_u(i, j),    i = I0+1+x, j = J0+1+y
+    __shared__ T rv[kNlTY + 2][kNlTX + 1];        // q_v(i, j),    i = I0+1+x, j = J0+1+y
+    __shared__ T rn[kNlTY][kNlTX];                // N2(i, j),     i = I0+1+x, j = J0+1+y
     const int tid = threadIdx.y * kNlTX + threadIdx.x;
     constexpr int NT = kNlTX * kNlBY;
     const double hc = gridstep(g, lev);
     // base_flux! of a static grid is U hc on every face (fluid.jl:22-32)
     const double sbx = prm_of()->fs[0] * hc, sby = prm_of()->fs[1] * hc;
     const bool moving = g.grid_moving;
+    // the tile's raw faces, Gamma and N2, all in flight at once (zeros outside the grid)
+#pragma unroll
+    for (int e = tid; e < (kNlTY + 1) * (kNlTX + 2); e += NT) {
+        const int x = e % (kNlTX + 2), y = e / (kNlTX + 2);
+        const int i = I0 + 1 + x, j = J0 + 1 + y;
+        if (i <= nx + 1 && j <= ny)
+            cp_async_elem(&ru[y][x], q + UI(i, j));
+        else
+            ru[y][x] = T(0);
+    }
+#pragma unroll
+    for (int e = tid; e < (kNlTY + 2) * (kNlTX + 1); e += NT) {
+        const int x = e % (kNlTX + 1), y = e / (kNlTX + 1);
+        const int i = I0 + 1 + x, j = J0 + 1 + y;
+        if (i <= nx && j <= ny + 1)
+            cp_async_elem(&rv[y][x], q + VI(i, j));
+        else
+            rv[y][x] = T(0);
+    }
+#pragma unroll
+    for (int e = tid; e < (kNlTY + 2) * (kNlTX + 2); e += NT) {
+        const int x = e % (kNlTX + 2), y = e / (kNlTX + 2);
+        const int i = I0 + x, j = J0 + y;
+        if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1)
+            cp_async_elem(&gm[y][x], Gt + GI(i, j));
+        else
+            gm[y][x] = T(0);
+    }
+    if (a.rest) {
+#pragma unroll
+        for (int e = tid; e < kNlTY * kNlTX; e += NT) {
+            const int x = e % kNlTX, y = e / kNlTX;
+            const int i = I0 + 1 + x, j = J0 + 1 + y;
+            if (i <= nx - 1 && j <= ny - 1)
+                cp_async_elem(&rn[y][x], a.n2 + b * ng + GI(i, j));
+            else
+                rn[y][x] = T(0);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // face averages Q = (q + q0) pair sums / 2 (avg_flux!), each formed once per tile
 #pragma unroll
     for (int e = tid; e < (kNlTY + 2) * kNlTX; e += NT) {
         const int x = e % kNlTX, y = e / kNlTX;
         const int i = I0 + 2 + x, j = J0 + 1 + y;
         double v = 0.0;
         if (i <= nx && j <= ny + 1) {
+            // q_v(i, j) = rv[y][x + 1], q_v(i - 1, j) = rv[y][x]
             if (moving)
-                v = avg_qy(a, prm_of(), q, nu, lev, i, j);
+                v = ((double)rv[y][x + 1] + (double)rv[y][x] + base_flux_y(g, prm_of(), lev, i, j) +
+                     base_flux_y(g, prm_of(), lev, i - 1, j)) / 2;
             else
-                v = ((double)q[VI(i, j)] + (double)q[VI(i - 1, j)] + sby + sby) / 2;
+                v = ((double)rv[y][x + 1] + (double)rv[y][x] + sby + sby) / 2;
         }
         aqy[y][x] = v;
     }
@@ -636,18 +669,14 @@ __global__ void __launch_bounds__(kNlTX *kNlBY, EXT ? 4 : 5) nonlinear_kernel(No
         const int i = I0 + 1 + x, j = J0 + 2 + y;
         double v = 0.0;
         if (i <= nx + 1 && j <= ny) {
+            // q_u(i, j) = ru[y + 1][x], q_u(i, j - 1) = ru[y][x]
             if (moving)
-                v = avg_qx(a, prm_of(), q, lev, i, j);
+                v = ((double)ru[y + 1][x] + (double)ru[y][x] + base_flux_x(g, prm_of(), lev, i, j) +
+                     base_flux_x(g, prm_of(), lev, i, j - 1)) / 2;
             else
-                v = ((double)q[UI(i, j)] + (double)q[UI(i, j - 1)] + sbx + sbx) / 2;
+                v = ((double)ru[y + 1][x] + (double)ru[y][x] + sbx + sbx) / 2;
         }
         aqx[y][x] = v;
-    }
-#pragma unroll
-    for (int e = tid; e < (kNlTY + 2) * (kNlTX + 2); e += NT) {
-        const int x = e % (kNlTX + 2), y = e / (kNlTX + 2);
-        const int i = I0 + x, j = J0 + y;
-        gm[y][x] = (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1) ? (double)Gt[GI(i, j)] : 0.0;
     }
     __syncthreads();
     const int x = threadIdx.x, I = I0 + 1 + x;
@@ -677,7 +706,7 @@ __global__ void __launch_bounds__(kNlTX *kNlBY, EXT ? 4 : 5) nonlinear_kernel(No
         a.out[b * ng + GI(I, J)] = (T)n1;
         if (a.rest) {
             // rest = dt b1 N1 + dt b2 N2 + rhsbc (fluid.jl:487-493), rhsbc = apply_bc!(0, get_bc(..); fac)
-            double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * (double)a.n2[b * ng + GI(I, J)];
+            double v = (g.dt * 1.5) * n1 + (g.dt * -0.5) * (double)rn[y][x];
             if (lev < g.L && on_ring(g, I, J)) {
                 const double fac = 0.25 * g.dt / (re_of() * (hc * hc));
                 v = v + apply_bc_at(0.0, C, g, I, J, fac);

@@ -81,11 +81,16 @@ class GpuCnabSolver(AbstractSolver):
         self._stale = False
         self.last_status = 0
 
-    def __del__(self):
+    def close(self):
+        """Frees the device state now (also done when the solver is collected).
+        An ensemble holding this solver then refuses to advance."""
         h = getattr(self, "_h", None)
         if h:
             self.lib.ibpm_destroy(h)
             self._h = None
+
+    def __del__(self):
+        self.close()
 
     def _view(self, s: State) -> _abi.ibpm_state_view:
         v = _abi.ibpm_state_view()

@@ -162,9 +162,11 @@ int ibpm_get_forces(ibpm_handle *h, double *fb, double *total_force);
  * enqueued before any is waited for; params[k * n + c] holds step k of case c.
  * Each case's results are the bits of stepping it alone.  While grouped, a
  * case's handle reads and writes its slot of the group's fields (its own
- * field buffers are freed); destroying the ensemble copies every case back
- * into buffers of its own, so destroy the ensemble before its handles.  A
- * handle may appear once.  The ensemble does not own the handles.  The
+ * field buffers are freed); destroying the ensemble copies every live case
+ * back into buffers of its own.  Handles and ensemble may be destroyed in
+ * either order: a handle destroyed first is dropped from its groups, and the
+ * ensemble then refuses to advance (IBPM_ERR_INVALID).  A handle may appear
+ * once.  The ensemble does not own the handles.  The
  * environment variable IBPM_ENSEMBLE_BATCH=0 at creation disables grouping
  * (every case on its own stream). */
 typedef struct ibpm_ensemble ibpm_ensemble;

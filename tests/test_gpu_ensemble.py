@@ -4,6 +4,10 @@ give the results of single steps when the host callbacks vary in time (the
 per-step parameters travel through pinned staging that is reused only after the
 copies that read it have run)."""
 import math
+import os
+import subprocess
+import sys
+import textwrap
 
 import numpy as np
 import pytest
@@ -33,6 +37,44 @@ def test_ensemble_matches_cases_stepped_alone(ib):
         assert np.array_equal(sa.q, sb.q)
         assert np.array_equal(a.total_force(), b.total_force())
         assert np.array_equal(sa.fb, sb.fb)
+
+
+def test_cases_destroyed_before_their_ensemble(ib):
+    probs = ib.configs.ensemble_cases(3, seed=7, h=0.04, widths=(64,), ny=64)
+    sol = [ib.GpuCnabSolver(ib.State(p), precision="fp32") for p in probs]
+    ens = ib.Ensemble(sol)
+    assert ens.groups() == (1, 3)
+    ens.advance_(2)
+    sol[0].close()  # the group's first case goes first
+    with pytest.raises(ib._abi.IbpmError):
+        ens.advance_(1)
+    ens.close()  # copies the live cases back; never touches the destroyed one
+    for s in sol[1:]:
+        s.advance_()
+        assert s.getstate().index == 3
+
+
+def test_interpreter_exit_with_a_live_ensemble():
+    # objects at module level with a module-level function form one reference
+    # cycle at exit, whose finalizers run in allocation order: every solver's
+    # before the ensemble's
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = textwrap.dedent(f"""
+        import sys
+        sys.path.insert(0, {os.path.join(root, "tests")!r})
+        from conftest import load_package
+        ib = load_package()
+        probs = ib.configs.ensemble_cases(3, seed=7, h=0.04, widths=(64, 96), ny=64)
+        sol = [ib.GpuCnabSolver(ib.State(p), precision="fp32") for p in probs]
+        ens = ib.Ensemble(sol)
+        def step():
+            ens.advance_(2)
+        step()
+        print("stepped")
+    """)
+    r = subprocess.run([sys.executable, "-X", "faulthandler", "-c", script], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0 and "stepped" in r.stdout, r.stderr[-2000:]
 
 
 def _gusty_cylinder(ib):
