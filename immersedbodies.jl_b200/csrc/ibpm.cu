@@ -777,16 +777,25 @@ struct Engine final : ibpm_handle {
     // computes q only at level 1 (the only level a caller reads).  win (device,
     // with curl_all=false): the level-1 faces the caller reads (E's support, the
     // body's bbox); level 1's last X pass and curl then skip what lies outside,
-    // leaving those rows of psi and faces of q unwritten.
+    // leaving those rows of psi and faces of q unwritten.  central: the coarse
+    // levels of Gm hold zeros outside the central block that coarsify! writes
+    // (a B application's vorticity), so their prologues and coarsening skip the
+    // loads there; the results are the same bits.
     void vort2flux(T *psi_, T *qout, T *Gm, long long bs, long long qbs, int nbatch, bool curl_all,
-                   bool hi1 = false, const int *win = nullptr) {
+                   bool hi1 = false, const int *win = nullptr, bool central = false) {
         if (curl_all) win = nullptr;
         for (int lev = 2; lev <= L; ++lev) {
             const int nx2 = nx / 2, ny2 = ny / 2;
             const dim3 blk(16, 16), grd((nx2 + 15) / 16, (ny2 + 15) / 16, nbatch);
-            coarsify_kernel<<<grd, blk, 0, st>>>(Gm + (lev - 1) * ng, Gm + (lev - 2) * ng, bs, g);
+            coarsify_kernel<<<grd, blk, 0, st>>>(Gm + (lev - 1) * ng, Gm + (lev - 2) * ng, bs, g,
+                                                 central && lev - 1 >= 2 ? 1 : 0);
             check_launch();
         }
+        // the central block coarsify! writes (faces nx/4+1 .. 3nx/4-1 by ny/4+1 .. 3ny/4-1)
+        auto centred = [&](const auto &in) {
+            using In = std::decay_t<decltype(in)>;
+            return InCentral<In>{in, nx / 4 + 1, 3 * nx / 4 - 1, ny / 4 + 1, 3 * ny / 4 - 1};
+        };
         for (int lev = L; lev >= 1; --lev) {
             T *Gl = Gm + (lev - 1) * ng;
             T *Pl = psi_ + (lev - 1) * ng;
@@ -813,19 +822,35 @@ struct Engine final : ibpm_handle {
                     // values read; level 1: the curl's window
                     TcKeep keep{TC_KEEP_LINES, nullptr, {ny / 4 - 1, 3 * ny / 4 - 1, nx / 4 - 1, 3 * nx / 4 - 1}};
                     if (lev == 1) keep = win ? TcKeep{TC_KEEP_WINDOW, win, {0, 0, 0, 0}} : TcKeep{TC_KEEP_ALL, nullptr, {0, 0, 0, 0}};
-                    if (lev == L)
-                        tc_solve(in_plain(Gl, bs), nbatch, tc_mult[0], Pl, bs, keep);
-                    else
-                        tc_solve(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, nbatch, tc_mult[0], Pl, bs,
-                                 keep);
+                    const bool cen = central && lev >= 2;
+                    if (lev == L) {
+                        if (cen)
+                            tc_solve(centred(in_plain(Gl, bs)), nbatch, tc_mult[0], Pl, bs, keep);
+                        else
+                            tc_solve(in_plain(Gl, bs), nbatch, tc_mult[0], Pl, bs, keep);
+                    } else {
+                        const InBC<T> in{Gl, psi_ + lev * ng, bs, bs, g};
+                        if (cen)
+                            tc_solve(centred(in), nbatch, tc_mult[0], Pl, bs, keep);
+                        else
+                            tc_solve(in, nbatch, tc_mult[0], Pl, bs, keep);
+                    }
                     solved = true;
                 }
             }
             if (!solved) {
-                if (lev == L)
-                    xpass(in_plain(Gl, bs), out_plain(t1, ng), nbatch);
-                else
-                    xpass(InBC<T>{Gl, psi_ + lev * ng, bs, bs, g}, out_plain(t1, ng), nbatch);
+                bool cen = false;
+                if constexpr (std::is_same<T, double>::value) cen = central && lev >= 2;
+                if (lev == L) {
+                    if constexpr (std::is_same<T, double>::value)
+                        if (cen) xpass(centred(in_plain(Gl, bs)), out_plain(t1, ng), nbatch);
+                    if (!cen) xpass(in_plain(Gl, bs), out_plain(t1, ng), nbatch);
+                } else {
+                    const InBC<T> in{Gl, psi_ + lev * ng, bs, bs, g};
+                    if constexpr (std::is_same<T, double>::value)
+                        if (cen) xpass(centred(in), out_plain(t1, ng), nbatch);
+                    if (!cen) xpass(in, out_plain(t1, ng), nbatch);
+                }
                 ypass(t1, t2, ng, nbatch, mult(MULT_LAPINV, 1, 0));
                 xpass(in_plain(t2, ng), out_plain(Pl, bs), nbatch, lev == 1 ? win : nullptr);
             }
@@ -871,7 +896,8 @@ struct Engine final : ibpm_handle {
             // writes them, so the zeros of the allocation stay
             xpass(in_plain(t2, ng), out_plain(Gw, ng * L), nbatch);
         }
-        vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false, false, P.bbox);  // E reads the bbox only
+        // E reads the bbox only; Gw's coarse levels are zero outside coarsify!'s block
+        vort2flux(psiw, qw, Gw, ng * L, nq, nbatch, false, false, P.bbox, true);
         launch_regT(P, qw, nq, x, xs, nbatch, 0, prm, g, st);
         check_launch();
     }

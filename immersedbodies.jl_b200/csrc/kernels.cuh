@@ -71,6 +71,28 @@ struct SplitRing<In, std::void_t<decltype(In::kSplitRing)>> {
     static constexpr bool value = In::kSplitRing;
 };
 
+// A prologue over a field that is zero outside the block i0..i1 x j0..j1: there
+// the field reads as zero without a load (the boundary values on the ring are
+// still added).  The coarse levels of a B application are such fields: their
+// vorticity is the finer level's coarsified into the central block
+// (coarsify!, src/fluid.jl:208-228), and zero elsewhere.
+template <class In>
+struct InCentral {
+    In in;
+    int i0, i1, j0, j1;
+    static constexpr bool kSplitRing = SplitRing<In>::value;
+    __device__ __forceinline__ bool inside(int i, int j) const { return i >= i0 && i <= i1 && j >= j0 && j <= j1; }
+    __device__ __forceinline__ double operator()(int b, int i, int j) const {
+        if constexpr (kSplitRing)
+            return inside(i, j) ? in(b, i, j) : in.ring(0.0, b, i, j);
+        else
+            return inside(i, j) ? in(b, i, j) : 0.0;
+    }
+    __device__ __forceinline__ double plain(int b, int i, int j) const { return inside(i, j) ? in.plain(b, i, j) : 0.0; }
+    __device__ __forceinline__ bool ring_row(int j) const { return in.ring_row(j); }
+    __device__ __forceinline__ double ring(double v, int b, int i, int j) const { return in.ring(v, b, i, j); }
+};
+
 // Prologue rot!(Gamma, reg!(q, f)) (src/fluid.jl:101-111 after src/coupling.jl:72-85),
 // evaluated from the regularised patch.
 template <class T>
@@ -781,8 +803,12 @@ __global__ void curl_kernel(T *__restrict__ qout, long long qbs, const TP *__res
 
 // coarsify! (src/fluid.jl:208-228): fine level -> central block of the next coarser level
 // (the fine level may be of another element type TF).
+// fine_central: the fine level is zero outside its own central block (faces
+// nx/4+1 .. 3nx/4-1 by ny/4+1 .. 3ny/4-1); stencils wholly outside it give zero
+// without a load.
 template <class T, class TF = T>
-__global__ void coarsify_kernel(T *__restrict__ coarse, const TF *__restrict__ fine, long long bs, Grid g) {
+__global__ void coarsify_kernel(T *__restrict__ coarse, const TF *__restrict__ fine, long long bs, Grid g,
+                                int fine_central = 0) {
     const int nx = g.nx, ny = g.ny;
     const int ni = (nx / 2 - 2 - (-nx / 2 + 2)) / 2 + 1, nic = (nx / 4 - 1) - (-nx / 4 + 1) + 1;
     const int nj = (ny / 2 - 2 - (-ny / 2 + 2)) / 2 + 1, njc = (ny / 4 - 1) - (-ny / 4 + 1) + 1;
@@ -794,6 +820,10 @@ __global__ void coarsify_kernel(T *__restrict__ coarse, const TF *__restrict__ f
     auto G = [&](long long k) -> double { return (double)Gf[k]; };
     const int i = nx / 2 + (-nx / 2 + 2) + 2 * a, ic = nx / 2 + (-nx / 4 + 1) + a;
     const int j = ny / 2 + (-ny / 2 + 2) + 2 * bb, jc = ny / 2 + (-ny / 4 + 1) + bb;
+    if (fine_central && (i + 1 < nx / 4 + 1 || i - 1 > 3 * nx / 4 - 1 || j + 1 < ny / 4 + 1 || j - 1 > 3 * ny / 4 - 1)) {
+        Gc[GI(ic, jc)] = (T)0.0;
+        return;
+    }
     Gc[GI(ic, jc)] = (T)(G(GI(i, j)) + 0.5 * (G(GI(i + 1, j)) + G(GI(i, j + 1)) + G(GI(i - 1, j)) + G(GI(i, j - 1))) +
                          0.25 * (G(GI(i + 1, j + 1)) + G(GI(i + 1, j - 1)) + G(GI(i - 1, j - 1)) + G(GI(i - 1, j + 1))));
 }
