@@ -439,8 +439,14 @@ __global__ void __launch_bounds__(D::TPF *NG, D::OCC / (D::TPF * NG))
 //   v = scale / Lambda_i * (S Gamma / Lambda_e + S rest)
 //     = (S Gamma (1 - lam c) + S rest) * scale / (1 + lam c),   c = dt / (2 Re hc^2);
 // phase 2 transforms the real v of two columns packed as one complex line.
+// Resident threads per SM the kernel is compiled for: 512 for FP32 lines of up to
+// 512 points (at most 128 registers a thread), 256 otherwise.
+template <class D>
+constexpr int trial_occ() {
+    return (sizeof(typename D::Real) == 4 && D::MC > 0 && D::MC <= 512) ? 512 : 256;
+}
 template <class D, int NG>
-__global__ void __launch_bounds__(D::TPF *NG, 256 / (D::TPF * NG))
+__global__ void __launch_bounds__(D::TPF *NG, trial_occ<D>() / (D::TPF * NG))
     ypass_trial_kernel(const typename D::Real *__restrict__ t1, const typename D::Real *__restrict__ t2,
                        typename D::Real *__restrict__ out, long long bs, int ncols, PlanT<typename D::Real> pl,
                        Mult mult) {
