@@ -392,7 +392,9 @@ __device__ __forceinline__ void stage_gen_first_pre(C *buf, const T *__restrict_
 template <int M, class T, class PL = Pow2Plan<M>>
 struct Pow2Dst {
     using P = PL;
-    static constexpr int OCC = P::OCC;
+    // FP32 lines of up to 256 points are compiled for twice the plan's resident
+    // threads (64 registers; the Y pass spills 32-52 bytes) -- measured faster
+    static constexpr int OCC = (sizeof(T) == 4 && M <= 256) ? 2 * P::OCC : P::OCC;
     static constexpr int MC = M;  // compile-time transform length
     using Real = T;
     using C = typename Cx<T>::type;
